@@ -1,0 +1,157 @@
+"""ctypes bindings for the oracle libraries (test infrastructure only).
+
+* :class:`RefLib` drives the reference's own C++ sources built by
+  ``make -C oracle ref`` (``oracle/_ref/libref_<variant>.so``) through the
+  ``extern "C"`` shim in ``oracle/ref_shim.cpp``.  Buffers use the
+  reference's layouts: decoder metrics per codeword are ``mcol`` columns of
+  ``(ceil(Z/P)+2)`` SIMD words, element ``j`` of column ``c`` at word
+  ``1 + c*(spz+2)`` (src/LDPCDec/decode_matrix_allocate.cpp:55,
+  src/Top/gen_metrics.cpp:37-39); codeword bits are one 512-bit word per
+  column, bit ``t`` = LSB-first (src/Top/gen_rand_databits.cpp:24-38).
+* :class:`Oracle` is the scalar C restatement (``oracle/liboracle.so``).
+
+Only tests, ``__graft_entry__.smoke`` and the CPU-baseline leg of
+``bench.py`` may use this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+_u32p = C.POINTER(C.c_uint32)
+
+
+def ref_available(variant: str = "Vec64c_min") -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "libref_%s.so" % variant))
+
+
+class RefLib:
+    """One reference build variant (e.g. ``Vec64c_min``, ``Vec16f_prod``)."""
+
+    def __init__(self, variant: str = "Vec64c_min"):
+        path = os.path.join(REF_DIR, "libref_%s.so" % variant)
+        # RTLD_LOCAL: every variant defines the same C++ symbols
+        self.lib = C.CDLL(path, mode=os.RTLD_LOCAL)
+        L = self.lib
+        L.ref_layout.argtypes = [C.POINTER(C.c_int)] * 4
+        L.ref_open.restype = C.c_void_p
+        L.ref_open.argtypes = [C.c_char_p, C.c_char_p, C.c_uint]
+        L.ref_dims.argtypes = [C.c_void_p] + [C.POINTER(C.c_uint)] * 5
+        L.ref_metrics.restype = C.c_void_p
+        L.ref_metrics.argtypes = [C.c_void_p]
+        L.ref_cw_bits.restype = C.c_void_p
+        L.ref_cw_bits.argtypes = [C.c_void_p]
+        L.ref_decode_set.restype = C.c_uint
+        L.ref_decode_set.argtypes = [C.c_void_p, C.c_uint, C.c_uint, C.c_uint, C.c_float, C.c_float]
+        L.ref_decode_each.restype = C.c_uint
+        L.ref_decode_each.argtypes = [C.c_void_p, C.c_uint, C.c_uint, C.c_float, C.c_float, _u32p]
+        L.ref_init_randstate.argtypes = [C.POINTER(C.c_uint64)]
+        L.ref_normdist2.argtypes = [C.POINTER(C.c_float), C.c_int]
+        L.ref_gen_rand_databits.argtypes = [C.c_void_p, C.c_uint]
+        L.ref_encode.argtypes = [C.c_void_p, C.c_uint]
+        L.ref_gen_metrics.restype = C.c_uint
+        L.ref_gen_metrics.argtypes = [C.c_void_p, C.c_uint, C.c_float, C.POINTER(C.c_float), C.c_float, C.c_float]
+        L.ref_count_errors.argtypes = [C.c_void_p, C.c_uint, _u32p, _u32p]
+        p, e, w, eb = (C.c_int(), C.c_int(), C.c_int(), C.c_int())
+        L.ref_layout(C.byref(p), C.byref(e), C.byref(w), C.byref(eb))
+        self.simd_par, self.elem_bw, self.width_bytes, self.enc_bytes = p.value, e.value, w.value, eb.value
+        self.dtype = {8: np.int8, 16: np.int16, 32: np.int32, -32: np.float32, -64: np.float64}[self.elem_bw]
+
+
+class RefCtx:
+    """Reference encoder+decoder state for one code and ``num_cw`` codewords."""
+
+    def __init__(self, lib: RefLib, code, num_cw: int):
+        self.lib, self.code, self.num_cw = lib, code, num_cw
+        self._tmp = tempfile.TemporaryDirectory()
+        enc = os.path.join(self._tmp.name, "LDPCencode.raw.dat")
+        dec = os.path.join(self._tmp.name, "LDPCdecode.raw.dat")
+        code.write_dat(enc, dec)
+        self.h = lib.lib.ref_open(enc.encode(), dec.encode(), num_cw)
+        z, mr, mc, npar, fc = (C.c_uint(), C.c_uint(), C.c_uint(), C.c_uint(), C.c_uint())
+        lib.lib.ref_dims(self.h, C.byref(z), C.byref(mr), C.byref(mc), C.byref(npar), C.byref(fc))
+        self.z, self.mrow, self.mcol = z.value, mr.value, mc.value
+        P = lib.simd_par
+        self.spz = (self.z + P - 1) // P
+        self.col_elems = (self.spz + 2) * P
+        itemsize = np.dtype(lib.dtype).itemsize
+        nelem = num_cw * self.mcol * self.col_elems
+        self.metrics = np.ctypeslib.as_array(
+            C.cast(lib.lib.ref_metrics(self.h), C.POINTER(C.c_uint8)), shape=(nelem * itemsize,)
+        ).view(lib.dtype).reshape(num_cw, self.mcol, self.col_elems)
+        self.cw_bits = np.ctypeslib.as_array(
+            C.cast(lib.lib.ref_cw_bits(self.h), C.POINTER(C.c_uint8)),
+            shape=(num_cw * self.mcol * lib.enc_bytes,)).reshape(num_cw, self.mcol, lib.enc_bytes)
+
+    # -- decoder input/output in the flat [cw][col*Z + t] view
+    def set_llr(self, llr: np.ndarray) -> None:
+        P = self.lib.simd_par
+        llr = np.asarray(llr).reshape(self.num_cw, self.mcol, self.z)
+        self.metrics[...] = 0
+        self.metrics[:, :, P:P + self.z] = llr
+
+    def posteriors(self) -> np.ndarray:
+        P = self.lib.simd_par
+        return self.metrics[:, :, P:P + self.z].reshape(self.num_cw, self.mcol * self.z).copy()
+
+    def decode_each(self, max_iter: int, max_row_metric: float, beta: float) -> np.ndarray:
+        it = np.zeros(self.num_cw, dtype=np.uint32)
+        self.lib.lib.ref_decode_each(self.h, self.num_cw, max_iter, max_row_metric, beta,
+                                     it.ctypes.data_as(_u32p))
+        return it
+
+    def decode_set(self, max_iter: int, max_row_metric: float, beta: float, first=0, count=None) -> int:
+        count = self.num_cw if count is None else count
+        return int(self.lib.lib.ref_decode_set(self.h, first, count, max_iter, max_row_metric, beta))
+
+    # -- encoder
+    def set_info_bits(self, bits: np.ndarray) -> None:
+        """bits: [num_cw][K_cols*Z] uint8 0/1 (data columns only)."""
+        kc = self.mcol - self.mrow
+        bits = np.asarray(bits, dtype=np.uint8).reshape(self.num_cw, kc, self.z)
+        self.cw_bits[...] = 0
+        packed = np.packbits(bits, axis=2, bitorder="little")
+        self.cw_bits[:, :kc, :packed.shape[2]] = packed
+
+    def codeword_bits(self) -> np.ndarray:
+        unp = np.unpackbits(self.cw_bits, axis=2, bitorder="little")[:, :, :self.z]
+        return unp.reshape(self.num_cw, self.mcol * self.z)
+
+    def encode(self) -> None:
+        self.lib.lib.ref_encode(self.h, self.num_cw)
+
+    def gen_rand_databits(self) -> None:
+        self.lib.lib.ref_gen_rand_databits(self.h, self.num_cw)
+
+    def gen_metrics(self, snr: float, wgn: np.ndarray, scale: float, max_abs: float) -> int:
+        wgn = np.ascontiguousarray(wgn, dtype=np.float32)
+        return int(self.lib.lib.ref_gen_metrics(self.h, self.num_cw, snr,
+                                                 wgn.ctypes.data_as(C.POINTER(C.c_float)), scale, max_abs))
+
+    def count_errors(self):
+        cw, bit = C.c_uint32(), C.c_uint32()
+        self.lib.lib.ref_count_errors(self.h, self.num_cw, C.byref(cw), C.byref(bit))
+        return cw.value, bit.value
+
+    def wgn_count(self) -> int:
+        """Number of Vec8f words of noise LDPCtop allocates per inner loop (LDPCtop.cpp:60-64)."""
+        n = self.num_cw * self.mcol * ((self.z + 7) // 8)
+        return n + (n & 1)
+
+
+def ref_init_randstate(lib: RefLib, seeds64) -> None:
+    s = np.ascontiguousarray(seeds64, dtype=np.uint64)
+    assert s.size == 64
+    lib.lib.ref_init_randstate(s.ctypes.data_as(C.POINTER(C.c_uint64)))
+
+
+def ref_normdist2(lib: RefLib, simd_count: int) -> np.ndarray:
+    out = np.zeros(simd_count * 8, dtype=np.float32)
+    lib.lib.ref_normdist2(out.ctypes.data_as(C.POINTER(C.c_float)), simd_count)
+    return out

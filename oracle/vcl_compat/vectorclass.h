@@ -1,0 +1,369 @@
+/* vectorclass.h -- compatibility header for building the reference's own
+ * C++ sources in this container (oracle / CPU-baseline only).
+ *
+ * The reference (tomt-1/simd-fecfun) is written against Agner Fog's
+ * "vectorclass" library, version 2 (github.com/vectorclass/version2; the
+ * reference pins no release: README.md:3,21, build/Makefile:5-7), which is not
+ * present here.  This header provides exactly the subset of that library's
+ * public API the reference calls, implemented from the library's documented
+ * semantics (manual "VCL version 2"):
+ *   - integer + - * wrap around; add_saturated/sub_saturated saturate;
+ *   - abs() of the most negative integer returns it unchanged;
+ *   - min/max of floats return the second operand when the first compares
+ *     false (as _mm_min_ps/_mm_max_ps do);
+ *   - roundi() rounds to nearest, ties to even;
+ *   - compress() truncates; load_partial() zero-fills; cutoff() zeroes tail;
+ *   - permuteN<i...>() with index -1 yields zero;
+ *   - mul_add() is a fused multiply-add.
+ * Lane-generic C++ with AVX-512BW fast paths for the 64 x int8 operations
+ * the decoder's inner loops use.  This is test infrastructure: nothing in
+ * the shipped library includes it.
+ */
+#ifndef VCL_COMPAT_VECTORCLASS_H
+#define VCL_COMPAT_VECTORCLASS_H
+
+#include <stdint.h>
+#include <string.h>
+#include <math.h>
+#include <type_traits>
+#include <immintrin.h>
+
+namespace vclc {
+
+template <int BYTES> struct Raw {
+    unsigned char b[BYTES];
+};
+
+template <int N> struct VecB {
+    bool m[N];
+    VecB() = default;
+    void load_bits(uint64_t bits) {
+        for (int i = 0; i < N; ++i) m[i] = (bits >> i) & 1;
+    }
+    friend uint64_t to_bits(const VecB& v) {
+        uint64_t r = 0;
+        for (int i = 0; i < N; ++i) r |= (uint64_t)v.m[i] << i;
+        return r;
+    }
+    friend VecB operator&(const VecB& a, const VecB& b) { VecB r; for (int i = 0; i < N; ++i) r.m[i] = a.m[i] && b.m[i]; return r; }
+    friend VecB operator|(const VecB& a, const VecB& b) { VecB r; for (int i = 0; i < N; ++i) r.m[i] = a.m[i] || b.m[i]; return r; }
+    friend VecB operator~(const VecB& a) { VecB r; for (int i = 0; i < N; ++i) r.m[i] = !a.m[i]; return r; }
+};
+
+template <class T> struct sat_lim {
+    static constexpr long long lo = std::is_signed<T>::value ? -(1LL << (8 * sizeof(T) - 1)) : 0;
+    static constexpr long long hi = std::is_signed<T>::value ? (1LL << (8 * sizeof(T) - 1)) - 1
+                                                            : (long long)((1ULL << (8 * sizeof(T))) - 1);
+};
+
+template <class T, int N>
+struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
+    static constexpr int BYTES = (int)sizeof(T) * N;
+    T e[N];
+
+    Vec() = default;
+    Vec(T v) { for (int i = 0; i < N; ++i) e[i] = v; }
+    Vec(const Raw<BYTES>& r) { memcpy(e, r.b, BYTES); }
+    template <class U, int M, class = typename std::enable_if<(int)sizeof(U) * M == BYTES && !(std::is_same<U, T>::value && M == N)>::type>
+    explicit Vec(const Vec<U, M>& o) { memcpy(e, o.e, BYTES); }
+    template <int H = N / 2, class = typename std::enable_if<(H * 2 == N && H >= 1)>::type>
+    Vec(const Vec<T, H>& lo, const Vec<T, H>& hi) { memcpy(e, lo.e, BYTES / 2); memcpy(e + H, hi.e, BYTES / 2); }
+    template <class... A, class = typename std::enable_if<(sizeof...(A) == N && N > 2)>::type>
+    Vec(A... a) { T t[N] = {(T)a...}; memcpy(e, t, BYTES); }
+
+    Vec& load(const void* p) { memcpy(e, p, BYTES); return *this; }
+    Vec& load_a(const void* p) { memcpy(e, p, BYTES); return *this; }
+    void store(void* p) const { memcpy(p, e, BYTES); }
+    void store_a(void* p) const { memcpy(p, e, BYTES); }
+    Vec& load_partial(int n, const void* p) {
+        if (n < 0) n = 0;
+        if (n > N) n = N;
+        memset(e, 0, BYTES);
+        memcpy(e, p, (size_t)n * sizeof(T));
+        return *this;
+    }
+    void store_partial(int n, void* p) const {
+        if (n < 0) n = 0;
+        if (n > N) n = N;
+        memcpy(p, e, (size_t)n * sizeof(T));
+    }
+    Vec& cutoff(int n) { for (int i = (n < 0 ? 0 : n); i < N; ++i) e[i] = 0; return *this; }
+    Vec& insert(int i, T v) { e[i & (N - 1)] = v; return *this; }
+    T extract(int i) const { return e[i & (N - 1)]; }
+    T operator[](int i) const { return e[i & (N - 1)]; }
+    static constexpr int size() { return N; }
+
+    /* ---- bitwise helpers on the raw bytes ---- */
+    template <class F> static Vec bitop(const Vec& a, const Vec& b, F f) {
+        Vec r; const unsigned char* pa = (const unsigned char*)a.e; const unsigned char* pb = (const unsigned char*)b.e;
+        unsigned char* pr = (unsigned char*)r.e;
+        for (int i = 0; i < BYTES; ++i) pr[i] = f(pa[i], pb[i]);
+        return r;
+    }
+
+    friend Vec operator&(const Vec& a, const Vec& b) {
+#if defined(__AVX512F__)
+        if constexpr (BYTES == 64) { Vec r; _mm512_storeu_si512(r.e, _mm512_and_si512(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r; }
+#endif
+        return bitop(a, b, [](unsigned char x, unsigned char y) { return (unsigned char)(x & y); });
+    }
+    friend Vec operator|(const Vec& a, const Vec& b) {
+#if defined(__AVX512F__)
+        if constexpr (BYTES == 64) { Vec r; _mm512_storeu_si512(r.e, _mm512_or_si512(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r; }
+#endif
+        return bitop(a, b, [](unsigned char x, unsigned char y) { return (unsigned char)(x | y); });
+    }
+    friend Vec operator^(const Vec& a, const Vec& b) {
+#if defined(__AVX512F__)
+        if constexpr (BYTES == 64) { Vec r; _mm512_storeu_si512(r.e, _mm512_xor_si512(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r; }
+#endif
+        return bitop(a, b, [](unsigned char x, unsigned char y) { return (unsigned char)(x ^ y); });
+    }
+    friend Vec operator~(const Vec& a) {
+        Vec r; const unsigned char* pa = (const unsigned char*)a.e; unsigned char* pr = (unsigned char*)r.e;
+        for (int i = 0; i < BYTES; ++i) pr[i] = (unsigned char)~pa[i];
+        return r;
+    }
+    friend Vec andnot(const Vec& a, const Vec& b) { return a & ~b; }
+    Vec& operator&=(const Vec& b) { *this = *this & b; return *this; }
+    Vec& operator|=(const Vec& b) { *this = *this | b; return *this; }
+    Vec& operator^=(const Vec& b) { *this = *this ^ b; return *this; }
+
+    /* ---- arithmetic ---- */
+    friend Vec operator+(const Vec& a, const Vec& b) {
+        Vec r;
+        if constexpr (std::is_integral<T>::value) {
+            using U = typename std::make_unsigned<T>::type;
+            for (int i = 0; i < N; ++i) r.e[i] = (T)(U)((U)a.e[i] + (U)b.e[i]);
+        } else {
+            for (int i = 0; i < N; ++i) r.e[i] = a.e[i] + b.e[i];
+        }
+        return r;
+    }
+    friend Vec operator-(const Vec& a, const Vec& b) {
+        Vec r;
+        if constexpr (std::is_integral<T>::value) {
+            using U = typename std::make_unsigned<T>::type;
+            for (int i = 0; i < N; ++i) r.e[i] = (T)(U)((U)a.e[i] - (U)b.e[i]);
+        } else {
+            for (int i = 0; i < N; ++i) r.e[i] = a.e[i] - b.e[i];
+        }
+        return r;
+    }
+    friend Vec operator*(const Vec& a, const Vec& b) {
+        Vec r;
+        if constexpr (std::is_integral<T>::value) {
+            using U = typename std::make_unsigned<T>::type;
+            for (int i = 0; i < N; ++i) r.e[i] = (T)(U)((U)a.e[i] * (U)b.e[i]);
+        } else {
+            for (int i = 0; i < N; ++i) r.e[i] = a.e[i] * b.e[i];
+        }
+        return r;
+    }
+    friend Vec operator/(const Vec& a, const Vec& b) { Vec r; for (int i = 0; i < N; ++i) r.e[i] = a.e[i] / b.e[i]; return r; }
+    friend Vec operator-(const Vec& a) { return Vec((T)0) - a; }
+    Vec& operator+=(const Vec& b) { *this = *this + b; return *this; }
+    Vec& operator-=(const Vec& b) { *this = *this - b; return *this; }
+    Vec& operator*=(const Vec& b) { *this = *this * b; return *this; }
+
+    friend Vec operator<<(const Vec& a, int s) {
+        Vec r; using U = typename std::make_unsigned<T>::type;
+        for (int i = 0; i < N; ++i) r.e[i] = (s >= (int)(8 * sizeof(T))) ? (T)0 : (T)(U)((U)a.e[i] << s);
+        return r;
+    }
+    friend Vec operator>>(const Vec& a, int s) {
+        Vec r;
+        for (int i = 0; i < N; ++i) {
+            if (s >= (int)(8 * sizeof(T))) r.e[i] = std::is_signed<T>::value ? (T)(a.e[i] < 0 ? -1 : 0) : (T)0;
+            else r.e[i] = (T)(a.e[i] >> s);   /* arithmetic for signed, logical for unsigned */
+        }
+        return r;
+    }
+
+    /* ---- comparisons ---- */
+    friend VecB<N> operator<(const Vec& a, const Vec& b) {
+        VecB<N> r;
+#if defined(__AVX512BW__)
+        if constexpr (std::is_same<T, int8_t>::value && N == 64) {
+            uint64_t m = _mm512_cmplt_epi8_mask(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e));
+            r.load_bits(m); return r;
+        }
+#endif
+        for (int i = 0; i < N; ++i) r.m[i] = a.e[i] < b.e[i];
+        return r;
+    }
+    friend VecB<N> operator>(const Vec& a, const Vec& b) { return b < a; }
+    friend VecB<N> operator<=(const Vec& a, const Vec& b) { VecB<N> r; for (int i = 0; i < N; ++i) r.m[i] = a.e[i] <= b.e[i]; return r; }
+    friend VecB<N> operator>=(const Vec& a, const Vec& b) { return b <= a; }
+    friend VecB<N> operator==(const Vec& a, const Vec& b) { VecB<N> r; for (int i = 0; i < N; ++i) r.m[i] = a.e[i] == b.e[i]; return r; }
+    friend VecB<N> operator!=(const Vec& a, const Vec& b) { VecB<N> r; for (int i = 0; i < N; ++i) r.m[i] = a.e[i] != b.e[i]; return r; }
+
+    /* ---- element functions ---- */
+    friend Vec select(const VecB<N>& s, const Vec& a, const Vec& b) {
+#if defined(__AVX512BW__)
+        if constexpr (std::is_same<T, int8_t>::value && N == 64) {
+            Vec r; _mm512_storeu_si512(r.e, _mm512_mask_blend_epi8((__mmask64)to_bits(s), _mm512_loadu_si512(b.e), _mm512_loadu_si512(a.e)));
+            return r;
+        }
+#endif
+        Vec r; for (int i = 0; i < N; ++i) r.e[i] = s.m[i] ? a.e[i] : b.e[i]; return r;
+    }
+    friend Vec if_sub(const VecB<N>& s, const Vec& a, const Vec& b) { return select(s, a - b, a); }
+    friend Vec if_add(const VecB<N>& s, const Vec& a, const Vec& b) { return select(s, a + b, a); }
+    friend Vec min(const Vec& a, const Vec& b) {
+#if defined(__AVX512BW__)
+        if constexpr (std::is_same<T, int8_t>::value && N == 64) {
+            Vec r; _mm512_storeu_si512(r.e, _mm512_min_epi8(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r;
+        }
+#endif
+        Vec r; for (int i = 0; i < N; ++i) r.e[i] = (a.e[i] < b.e[i]) ? a.e[i] : b.e[i]; return r;
+    }
+    friend Vec max(const Vec& a, const Vec& b) {
+#if defined(__AVX512BW__)
+        if constexpr (std::is_same<T, int8_t>::value && N == 64) {
+            Vec r; _mm512_storeu_si512(r.e, _mm512_max_epi8(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r;
+        }
+#endif
+        Vec r; for (int i = 0; i < N; ++i) r.e[i] = (a.e[i] > b.e[i]) ? a.e[i] : b.e[i]; return r;
+    }
+    friend Vec abs(const Vec& a) {
+        Vec r;
+        if constexpr (std::is_integral<T>::value) {
+#if defined(__AVX512BW__)
+            if constexpr (std::is_same<T, int8_t>::value && N == 64) {
+                _mm512_storeu_si512(r.e, _mm512_abs_epi8(_mm512_loadu_si512(a.e))); return r;
+            }
+#endif
+            using U = typename std::make_unsigned<T>::type;
+            for (int i = 0; i < N; ++i) r.e[i] = (a.e[i] < 0) ? (T)(U)(0u - (U)a.e[i]) : a.e[i];
+        } else {
+            for (int i = 0; i < N; ++i) r.e[i] = fabs(a.e[i]);
+        }
+        return r;
+    }
+    friend Vec add_saturated(const Vec& a, const Vec& b) {
+#if defined(__AVX512BW__)
+        if constexpr (std::is_same<T, int8_t>::value && N == 64) {
+            Vec r; _mm512_storeu_si512(r.e, _mm512_adds_epi8(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r;
+        }
+#endif
+        Vec r;
+        for (int i = 0; i < N; ++i) {
+            long long v = (long long)a.e[i] + (long long)b.e[i];
+            r.e[i] = (T)(v < sat_lim<T>::lo ? sat_lim<T>::lo : v > sat_lim<T>::hi ? sat_lim<T>::hi : v);
+        }
+        return r;
+    }
+    friend Vec sub_saturated(const Vec& a, const Vec& b) {
+#if defined(__AVX512BW__)
+        if constexpr (std::is_same<T, int8_t>::value && N == 64) {
+            Vec r; _mm512_storeu_si512(r.e, _mm512_subs_epi8(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r;
+        }
+#endif
+        Vec r;
+        for (int i = 0; i < N; ++i) {
+            long long v = (long long)a.e[i] - (long long)b.e[i];
+            r.e[i] = (T)(v < sat_lim<T>::lo ? sat_lim<T>::lo : v > sat_lim<T>::hi ? sat_lim<T>::hi : v);
+        }
+        return r;
+    }
+    friend Vec mul_add(const Vec& a, const Vec& b, const Vec& c) {
+        Vec r;
+        if constexpr (std::is_same<T, float>::value) { for (int i = 0; i < N; ++i) r.e[i] = fmaf(a.e[i], b.e[i], c.e[i]); }
+        else if constexpr (std::is_same<T, double>::value) { for (int i = 0; i < N; ++i) r.e[i] = fma(a.e[i], b.e[i], c.e[i]); }
+        else { r = a * b + c; }
+        return r;
+    }
+    friend Vec sqrt(const Vec& a) {
+        Vec r;
+        if constexpr (std::is_same<T, float>::value) { for (int i = 0; i < N; ++i) r.e[i] = sqrtf(a.e[i]); }
+        else { for (int i = 0; i < N; ++i) r.e[i] = (T)::sqrt((double)a.e[i]); }
+        return r;
+    }
+    friend T horizontal_add(const Vec& a) {
+        if constexpr (std::is_integral<T>::value) {
+            using U = typename std::make_unsigned<T>::type;
+            U s = 0; for (int i = 0; i < N; ++i) s = (U)(s + (U)a.e[i]); return (T)s;
+        } else {
+            T s = 0; for (int i = 0; i < N; ++i) s += a.e[i]; return s;
+        }
+    }
+};
+
+template <class T, int N> Raw<(int)sizeof(T) * N> reinterpret_i(const Vec<T, N>& a) { Raw<(int)sizeof(T) * N> r; memcpy(r.b, a.e, sizeof(r.b)); return r; }
+template <class T, int N> Raw<(int)sizeof(T) * N> reinterpret_f(const Vec<T, N>& a) { Raw<(int)sizeof(T) * N> r; memcpy(r.b, a.e, sizeof(r.b)); return r; }
+template <int B> Raw<B> reinterpret_i(const Raw<B>& a) { return a; }
+template <int B> Raw<B> reinterpret_f(const Raw<B>& a) { return a; }
+
+template <int N> Vec<float, N> to_float(const Vec<int32_t, N>& a) { Vec<float, N> r; for (int i = 0; i < N; ++i) r.e[i] = (float)a.e[i]; return r; }
+template <int N> Vec<float, N> to_float(const Vec<uint32_t, N>& a) { Vec<float, N> r; for (int i = 0; i < N; ++i) r.e[i] = (float)a.e[i]; return r; }
+template <int N> Vec<double, N> to_double(const Vec<float, N>& a) { Vec<double, N> r; for (int i = 0; i < N; ++i) r.e[i] = (double)a.e[i]; return r; }
+template <int N> Vec<int32_t, N> roundi(const Vec<float, N>& a) { Vec<int32_t, N> r; for (int i = 0; i < N; ++i) r.e[i] = (int32_t)nearbyintf(a.e[i]); return r; }
+template <int N> Vec<int32_t, N> truncatei(const Vec<float, N>& a) { Vec<int32_t, N> r; for (int i = 0; i < N; ++i) r.e[i] = (int32_t)a.e[i]; return r; }
+template <int N> Vec<int16_t, N> compress(const Vec<int32_t, N>& a) { Vec<int16_t, N> r; for (int i = 0; i < N; ++i) r.e[i] = (int16_t)(uint16_t)(uint32_t)a.e[i]; return r; }
+
+template <class T, int N, int... I> Vec<T, N> permute_impl(const Vec<T, N>& a) {
+    static_assert(sizeof...(I) == N, "permute needs one index per element");
+    const int idx[N] = {I...};
+    Vec<T, N> r;
+    for (int i = 0; i < N; ++i) r.e[i] = (idx[i] < 0) ? (T)0 : a.e[idx[i]];
+    return r;
+}
+template <int... I, class T> Vec<T, 4> permute4(const Vec<T, 4>& a) { return permute_impl<T, 4, I...>(a); }
+template <int... I, class T> Vec<T, 8> permute8(const Vec<T, 8>& a) { return permute_impl<T, 8, I...>(a); }
+template <int... I, class T> Vec<T, 16> permute16(const Vec<T, 16>& a) { return permute_impl<T, 16, I...>(a); }
+
+} /* namespace vclc */
+
+typedef vclc::Vec<int8_t, 16> Vec16c;
+typedef vclc::Vec<int8_t, 32> Vec32c;
+typedef vclc::Vec<int8_t, 64> Vec64c;
+typedef vclc::Vec<int16_t, 8> Vec8s;
+typedef vclc::Vec<int16_t, 16> Vec16s;
+typedef vclc::Vec<int16_t, 32> Vec32s;
+typedef vclc::Vec<int32_t, 4> Vec4i;
+typedef vclc::Vec<int32_t, 8> Vec8i;
+typedef vclc::Vec<int32_t, 16> Vec16i;
+typedef vclc::Vec<uint32_t, 8> Vec8ui;
+typedef vclc::Vec<uint32_t, 16> Vec16ui;
+typedef vclc::Vec<int64_t, 4> Vec4q;
+typedef vclc::Vec<int64_t, 8> Vec8q;
+typedef vclc::Vec<uint64_t, 4> Vec4uq;
+typedef vclc::Vec<uint64_t, 8> Vec8uq;
+typedef vclc::Vec<float, 8> Vec8f;
+typedef vclc::Vec<float, 16> Vec16f;
+typedef vclc::Vec<double, 4> Vec4d;
+typedef vclc::Vec<double, 8> Vec8d;
+typedef vclc::VecB<8> Vec8fb;
+typedef vclc::VecB<8> Vec8ib;
+typedef vclc::VecB<16> Vec16fb;
+typedef vclc::VecB<16> Vec16ib;
+typedef vclc::VecB<16> Vec16cb;
+typedef vclc::VecB<32> Vec32cb;
+typedef vclc::VecB<64> Vec64cb;
+
+/* sign_combine(a, b) for float vectors: a with its sign bit flipped where b
+ * has the sign bit set (the integer overloads are in the reference's own
+ * vectorclass_extensions.h). */
+template <class V> static inline V vclc_sign_combine_f(const V& a, const V& b) {
+    V r;
+    for (int i = 0; i < V::size(); ++i) r.e[i] = std::signbit(b.e[i]) ? -a.e[i] : a.e[i];
+    return r;
+}
+static inline Vec8f sign_combine(const Vec8f a, const Vec8f b) { return vclc_sign_combine_f(a, b); }
+static inline Vec16f sign_combine(const Vec16f a, const Vec16f b) { return vclc_sign_combine_f(a, b); }
+static inline Vec4d sign_combine(const Vec4d a, const Vec4d b) { return vclc_sign_combine_f(a, b); }
+static inline Vec8d sign_combine(const Vec8d a, const Vec8d b) { return vclc_sign_combine_f(a, b); }
+
+using vclc::permute4;
+using vclc::permute8;
+using vclc::permute16;
+using vclc::to_float;
+using vclc::to_double;
+using vclc::roundi;
+using vclc::truncatei;
+using vclc::compress;
+using vclc::reinterpret_i;
+using vclc::reinterpret_f;
+
+#endif /* VCL_COMPAT_VECTORCLASS_H */

@@ -1,0 +1,24 @@
+/* vectormath_hyp.h -- compatibility header (oracle / CPU-baseline only).
+ *
+ * The reference's sum-product tree (src/LDPCDec/min_find.pl:37-48,98-106)
+ * calls tanh() and atanh() on float vectors from vectorclass's
+ * vectormath_hyp.h, which is absent here.  Both are mapped lane by lane onto
+ * the project's shared float functions (simd-fecfun_b200/csrc/ldpc_math.h),
+ * the same code the GPU decoder runs, so the CPU oracle and the GPU agree
+ * bit for bit.  This pins parity to that function, not to vectorclass's.
+ */
+#ifndef VCL_COMPAT_VECTORMATH_HYP_H
+#define VCL_COMPAT_VECTORMATH_HYP_H
+#include "vectorclass.h"
+#include "ldpc_math.h"
+
+template <class V> static inline V vclc_lanewise(const V& a, float (*f)(float)) {
+    V r;
+    for (int i = 0; i < V::size(); ++i) r.e[i] = f(a.e[i]);
+    return r;
+}
+static inline Vec8f tanh(const Vec8f a) { return vclc_lanewise(a, lm_tanh); }
+static inline Vec16f tanh(const Vec16f a) { return vclc_lanewise(a, lm_tanh); }
+static inline Vec8f atanh(const Vec8f a) { return vclc_lanewise(a, lm_atanh); }
+static inline Vec16f atanh(const Vec16f a) { return vclc_lanewise(a, lm_atanh); }
+#endif
