@@ -1,0 +1,297 @@
+/* ldpc_oracle.c -- scalar CPU restatement of the reference's LDPC hot path.
+ * TEST INFRASTRUCTURE ONLY (see ldpc_oracle.h).  Parity pinned against the
+ * reference's own decoder sources built in oracle/_ref (tests/test_oracle.py).
+ */
+#include "ldpc_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "ldpc_math.h"
+
+/* ---- int8 element semantics of the reference's Vec64c operations ---- */
+static int8_t sat8(int v) { return (int8_t)(v < -128 ? -128 : v > 127 ? 127 : v); }
+static int8_t wrap8(int v) { return (int8_t)(uint8_t)(v & 0xff); }
+/* vectorclass abs(): the most negative value maps to itself */
+static int8_t abs8(int8_t q) { return q < 0 ? wrap8(-(int)q) : q; }
+
+/* decode_row's Max_row_simd (decode_functions.cpp:27-32) for an int8 build */
+static int8_t max_row_i8(float max_row_metric) {
+    if (max_row_metric < 1e-6) return (int8_t)(1.0 - (double)(int8_t)max_row_metric);
+    return (int8_t)max_row_metric;
+}
+static float max_row_f32(float max_row_metric) {
+    if (max_row_metric < 1e-6) return (float)(1.0 - (double)max_row_metric);
+    return max_row_metric;
+}
+
+static int total_edges(const orc_code *c) {
+    int e = 0;
+    for (int r = 0; r < c->mrow; ++r) e += c->row_weights[r];
+    return e;
+}
+
+static int max_weight(const orc_code *c) {
+    int m = 0;
+    for (int r = 0; r < c->mrow; ++r) if (c->row_weights[r] > m) m = c->row_weights[r];
+    return m;
+}
+
+/* Evaluate a tree program (trees.py flat format) on the row's inputs.
+ * kind: 0 = int8 min, 1 = float min, 2 = float product.  */
+static void run_tree_i8(const int32_t *prog, int len, int d, const int8_t *in, int8_t maxv, int8_t *node, int8_t *out) {
+    for (int j = 0; j < d; ++j) node[j] = in[j];
+    for (int k = 0; k < len; ++k) {
+        const int32_t *q = prog + 4 * k;
+        if (q[0] == 0) node[q[1]] = node[q[2]] < node[q[3]] ? node[q[2]] : node[q[3]];
+        else if (q[0] == 1) node[q[1]] = maxv < node[q[1]] ? maxv : node[q[1]];
+        else out[q[1]] = node[q[2]];
+    }
+}
+
+static void run_tree_f32(const int32_t *prog, int len, int d, int prod, const float *in, float maxv, float *node, float *out) {
+    for (int j = 0; j < d; ++j) node[j] = in[j];
+    for (int k = 0; k < len; ++k) {
+        const int32_t *q = prog + 4 * k;
+        if (q[0] == 0) {
+            float a = node[q[2]], b = node[q[3]];
+            node[q[1]] = prod ? a * b : (a < b ? a : b);
+        } else if (q[0] == 1) {
+            node[q[1]] = maxv < node[q[1]] ? maxv : node[q[1]];
+        } else {
+            out[q[1]] = node[q[2]];
+        }
+    }
+}
+
+/* the int8 program for weight d: reuse the float program layout passed in by
+ * the caller (same schedule) */
+static const orc_trees *g_trees_i8 = 0;
+
+int orc_decode_int8(const orc_code *c, const int8_t *llr, size_t n_cw, unsigned max_iter,
+                    float max_row_metric, float beta, int8_t *post_out, uint32_t *iters_out) {
+    const int z = c->z, n = z * c->mcol, E = total_edges(c), dmax = max_weight(c);
+    const int8_t beta8 = (int8_t)beta, maxv = max_row_i8(max_row_metric);
+    int8_t *P = (int8_t *)malloc((size_t)n);
+    int8_t *R = (int8_t *)malloc((size_t)E * z);
+    int8_t *Q = (int8_t *)malloc((size_t)dmax), *m = (int8_t *)malloc((size_t)dmax);
+    int8_t *f = (int8_t *)malloc((size_t)dmax), *node = (int8_t *)malloc((size_t)dmax * 8 + 64);
+    int *v = (int *)malloc(sizeof(int) * (size_t)dmax);
+    for (size_t cw = 0; cw < n_cw; ++cw) {
+        memcpy(P, llr + cw * (size_t)n, (size_t)n);
+        memset(R, 0, (size_t)E * z);
+        unsigned iter = 0;
+        int done = 0;
+        while (!done) {
+            int e0 = 0;
+            for (int r = 0; r < c->mrow; ++r) {
+                const int d = c->row_weights[r];
+                for (int t = 0; t < z; ++t) {
+                    int8_t rx = 0;
+                    for (int j = 0; j < d; ++j) {
+                        const int col = c->row_cols[e0 + j], s = c->row_shifts[e0 + j];
+                        v[j] = col * z + (s + t) % z;
+                        Q[j] = sat8((int)P[v[j]] - (int)R[(size_t)(e0 + j) * z + t]);
+                        int8_t a = wrap8((int)abs8(Q[j]) - (int)beta8);
+                        m[j] = a > 0 ? a : 0;
+                        rx ^= Q[j];
+                    }
+                    if (g_trees_i8) {
+                        run_tree_i8(g_trees_i8->prog + 4 * g_trees_i8->off[d], g_trees_i8->len[d], d, m, maxv, node, f);
+                    } else {
+                        for (int j = 0; j < d; ++j) {
+                            int8_t mn = maxv;
+                            for (int k = 0; k < d; ++k) if (k != j && m[k] < mn) mn = m[k];
+                            f[j] = mn;
+                        }
+                    }
+                    for (int j = 0; j < d; ++j) {
+                        int8_t s = (int8_t)(rx ^ Q[j]);
+                        int8_t rn = s < 0 ? wrap8(-(int)f[j]) : f[j];
+                        P[v[j]] = sat8((int)Q[j] + (int)rn);
+                        R[(size_t)(e0 + j) * z + t] = rn;
+                    }
+                }
+                e0 += d;
+            }
+            /* syndrome on the posteriors after the full iteration */
+            int bad = 0;
+            e0 = 0;
+            for (int r = 0; r < c->mrow && !bad; ++r) {
+                const int d = c->row_weights[r];
+                for (int t = 0; t < z; ++t) {
+                    int8_t x = 0;
+                    for (int j = 0; j < d; ++j) x ^= P[c->row_cols[e0 + j] * z + (c->row_shifts[e0 + j] + t) % z];
+                    if (x < 0) { bad = 1; break; }
+                }
+                e0 += d;
+            }
+            ++iter;
+            done = !bad || iter == max_iter;
+        }
+        if (post_out) memcpy(post_out + cw * (size_t)n, P, (size_t)n);
+        if (iters_out) iters_out[cw] = iter;
+    }
+    free(P); free(R); free(Q); free(m); free(f); free(node); free(v);
+    return 0;
+}
+
+static uint32_t fbits(float x) { uint32_t u; memcpy(&u, &x, 4); return u; }
+static float bitsf(uint32_t u) { float x; memcpy(&x, &u, 4); return x; }
+
+int orc_decode_f32(const orc_code *c, const orc_trees *tr, int mode, const float *llr, size_t n_cw,
+                   unsigned max_iter, float max_row_metric, float beta, float *post_out, uint32_t *iters_out) {
+    const int z = c->z, n = z * c->mcol, E = total_edges(c), dmax = max_weight(c);
+    const float maxv = max_row_f32(max_row_metric);
+    if (dmax > tr->max_d) return -1;
+    float *P = (float *)malloc(sizeof(float) * (size_t)n);
+    float *R = (float *)malloc(sizeof(float) * (size_t)E * z);
+    float *Q = (float *)malloc(sizeof(float) * (size_t)dmax), *x = (float *)malloc(sizeof(float) * (size_t)dmax);
+    float *f = (float *)malloc(sizeof(float) * (size_t)dmax), *node = (float *)malloc(sizeof(float) * ((size_t)dmax * 8 + 64));
+    int *v = (int *)malloc(sizeof(int) * (size_t)dmax);
+    for (size_t cw = 0; cw < n_cw; ++cw) {
+        memcpy(P, llr + cw * (size_t)n, sizeof(float) * (size_t)n);
+        memset(R, 0, sizeof(float) * (size_t)E * z);
+        unsigned iter = 0;
+        int done = 0;
+        while (!done) {
+            int e0 = 0;
+            for (int r = 0; r < c->mrow; ++r) {
+                const int d = c->row_weights[r];
+                for (int t = 0; t < z; ++t) {
+                    uint32_t rx = 0;
+                    for (int j = 0; j < d; ++j) {
+                        const int col = c->row_cols[e0 + j], s = c->row_shifts[e0 + j];
+                        v[j] = col * z + (s + t) % z;
+                        Q[j] = P[v[j]] - R[(size_t)(e0 + j) * z + t];
+                        float a = fabsf(Q[j]) - beta;
+                        a = a > 0.0f ? a : 0.0f;
+                        x[j] = mode ? lm_tanh(a * 0.5f) : a;
+                        rx ^= fbits(Q[j]);
+                    }
+                    run_tree_f32(tr->prog + 4 * tr->off[d], tr->len[d], d, mode, x, maxv, node, f);
+                    for (int j = 0; j < d; ++j) {
+                        float fj = mode ? 2.0f * lm_atanh(f[j]) : f[j];
+                        uint32_t s = rx ^ fbits(Q[j]);
+                        float rn = (s & 0x80000000u) ? bitsf(fbits(fj) ^ 0x80000000u) : fj;
+                        P[v[j]] = Q[j] + rn;
+                        R[(size_t)(e0 + j) * z + t] = rn;
+                    }
+                }
+                e0 += d;
+            }
+            int bad = 0;
+            e0 = 0;
+            for (int r = 0; r < c->mrow && !bad; ++r) {
+                const int d = c->row_weights[r];
+                for (int t = 0; t < z; ++t) {
+                    uint32_t xx = 0;
+                    for (int j = 0; j < d; ++j) xx ^= fbits(P[c->row_cols[e0 + j] * z + (c->row_shifts[e0 + j] + t) % z]);
+                    if (xx & 0x80000000u) { bad = 1; break; }
+                }
+                e0 += d;
+            }
+            ++iter;
+            done = !bad || iter == max_iter;
+        }
+        if (post_out) memcpy(post_out + cw * (size_t)n, P, sizeof(float) * (size_t)n);
+        if (iters_out) iters_out[cw] = iter;
+    }
+    free(P); free(R); free(Q); free(x); free(f); free(node); free(v);
+    return 0;
+}
+
+/* int8 decoding through the generated min tree instead of the direct
+ * exclusive minimum (identical by exactness of integer min; kept to check it) */
+int orc_decode_int8_tree(const orc_code *c, const orc_trees *tr, const int8_t *llr, size_t n_cw,
+                         unsigned max_iter, float max_row_metric, float beta, int8_t *post_out,
+                         uint32_t *iters_out) {
+    g_trees_i8 = tr;
+    int rc = orc_decode_int8(c, llr, n_cw, max_iter, max_row_metric, beta, post_out, iters_out);
+    g_trees_i8 = 0;
+    return rc;
+}
+
+void orc_sigma(float snr, float llr_scale, float *sigma, float *sigma_factor) {
+    float three_db = 10 * log10f(2.0);
+    float s = powf(10.0, ((snr + three_db) / -20.0));
+    *sigma = s;
+    *sigma_factor = 2 * llr_scale / (s * s);
+}
+
+int orc_llr(int bit, float noise, float sigma, float sigma_factor, float max_abs, int punct, int filler,
+            float *llr_f, int32_t *llr_i) {
+    float orig = bit ? -1.0f : 1.0f;
+    float rx = fmaf(noise, sigma, orig);
+    int err = (int)((fbits(orig) ^ fbits(rx)) >> 31);
+    float l = rx * sigma_factor;
+    l = max_abs < l ? max_abs : l;
+    l = -max_abs > l ? -max_abs : l;
+    if (punct) l = 0.0f;
+    if (filler) l = max_abs;
+    if (llr_f) *llr_f = l;
+    if (llr_i) *llr_i = (int32_t)nearbyintf(l);
+    return err;
+}
+
+void orc_encode(int z, int mcol, int mrow, const int32_t *sched, int n_par, const uint8_t *info,
+                size_t n_cw, uint8_t *cw) {
+    const int kc = mcol - mrow, n = z * mcol;
+    uint8_t *acc = (uint8_t *)malloc((size_t)z);
+    for (size_t w = 0; w < n_cw; ++w) {
+        uint8_t *x = cw + w * (size_t)n;
+        memset(x, 0, (size_t)n);
+        memcpy(x, info + w * (size_t)kc * z, (size_t)kc * z);
+        const int32_t *p = sched;
+        for (int k = 0; k < n_par; ++k) {
+            int pc = p[0], cnt = p[1];
+            memset(acc, 0, (size_t)z);
+            for (int i = 0; i < cnt; ++i) {
+                int col = p[2 + 2 * i], sh = p[3 + 2 * i];
+                for (int t = 0; t < z; ++t) acc[t] ^= x[col * z + (t + sh) % z];
+            }
+            memcpy(x + pc * z, acc, (size_t)z);
+            p += 2 + 2 * cnt;
+        }
+    }
+    free(acc);
+}
+
+static void count_core(int z, int mcol, int mrow, int num_par, const uint8_t *hard, const uint8_t *sent,
+                       uint64_t *cw_err, uint64_t *bit_err) {
+    int slot_err[64];
+    uint64_t bits = 0;
+    memset(slot_err, 0, sizeof(slot_err));
+    for (int c = 0; c < mcol - mrow; ++c)
+        for (int t = 0; t < z; ++t)
+            if (hard[c * z + t] != sent[c * z + t]) { ++bits; slot_err[t % num_par] = 1; }
+    if (bits) {
+        for (int p = 0; p < num_par; ++p) *cw_err += (uint64_t)slot_err[p];
+        *bit_err += bits;
+    }
+}
+
+void orc_count_errors_i8(int z, int mcol, int mrow, int num_par, const int8_t *post, const uint8_t *cw_bits,
+                         size_t n_cw, uint64_t *cw_err, uint64_t *bit_err) {
+    const int n = z * mcol;
+    uint8_t *hard = (uint8_t *)malloc((size_t)n);
+    *cw_err = 0; *bit_err = 0;
+    for (size_t w = 0; w < n_cw; ++w) {
+        for (int i = 0; i < n; ++i) hard[i] = post[w * (size_t)n + i] < 0;
+        count_core(z, mcol, mrow, num_par, hard, cw_bits + w * (size_t)n, cw_err, bit_err);
+    }
+    free(hard);
+}
+
+void orc_count_errors_f32(int z, int mcol, int mrow, int num_par, const float *post, const uint8_t *cw_bits,
+                          size_t n_cw, uint64_t *cw_err, uint64_t *bit_err) {
+    const int n = z * mcol;
+    uint8_t *hard = (uint8_t *)malloc((size_t)n);
+    *cw_err = 0; *bit_err = 0;
+    for (size_t w = 0; w < n_cw; ++w) {
+        for (int i = 0; i < n; ++i) hard[i] = post[w * (size_t)n + i] < 0.0f;
+        count_core(z, mcol, mrow, num_par, hard, cw_bits + w * (size_t)n, cw_err, bit_err);
+    }
+    free(hard);
+}

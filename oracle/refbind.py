@@ -155,3 +155,128 @@ def ref_normdist2(lib: RefLib, simd_count: int) -> np.ndarray:
     out = np.zeros(simd_count * 8, dtype=np.float32)
     lib.lib.ref_normdist2(out.ctypes.data_as(C.POINTER(C.c_float)), simd_count)
     return out
+
+
+class Oracle:
+    """The scalar C restatement (``oracle/liboracle.so``)."""
+
+    def __init__(self):
+        self.lib = C.CDLL(os.path.join(HERE, "liboracle.so"))
+        self._trees = None
+
+    class _Code(C.Structure):
+        _fields_ = [("z", C.c_int), ("mrow", C.c_int), ("mcol", C.c_int),
+                    ("row_weights", C.POINTER(C.c_int32)), ("row_cols", C.POINTER(C.c_int32)),
+                    ("row_shifts", C.POINTER(C.c_int32))]
+
+    class _Trees(C.Structure):
+        _fields_ = [("prog", C.POINTER(C.c_int32)), ("off", C.POINTER(C.c_int32)),
+                    ("len", C.POINTER(C.c_int32)), ("max_d", C.c_int)]
+
+    def _code(self, code):
+        d = code.dec
+        keep = [np.ascontiguousarray(d[k], dtype=np.int32) for k in ("row_weights", "row_cols", "row_shifts")]
+        p = C.POINTER(C.c_int32)
+        s = self._Code(code.z, code.mrow, code.mcol, *(a.ctypes.data_as(p) for a in keep))
+        return s, keep
+
+    def _tree_struct(self):
+        if self._trees is None:
+            import sys
+            sys.path.insert(0, os.path.join(os.path.dirname(HERE), "simd-fecfun_b200"))
+            from ldpc_b200 import trees
+            prog, off, ln = [], [0] * 54, [0] * 54
+            for d in range(2, 54):
+                fp = trees.flat_program(d)
+                off[d] = len(prog) // 4
+                ln[d] = len(fp) // 4
+                prog += fp
+            keep = [np.array(prog, np.int32), np.array(off, np.int32), np.array(ln, np.int32)]
+            p = C.POINTER(C.c_int32)
+            self._trees = (self._Trees(keep[0].ctypes.data_as(p), keep[1].ctypes.data_as(p),
+                                       keep[2].ctypes.data_as(p), 53), keep)
+        return self._trees[0]
+
+    def decode_int8(self, code, llr, max_iter=10, max_row_metric=31.0, beta=1.0, use_tree=False):
+        llr = np.ascontiguousarray(llr, dtype=np.int8).reshape(-1, code.n)
+        n = llr.shape[0]
+        post = np.zeros_like(llr)
+        it = np.zeros(n, np.uint32)
+        cs, keep = self._code(code)
+        if use_tree:
+            self.lib.orc_decode_int8_tree(C.byref(cs), C.byref(self._tree_struct()), llr.ctypes.data_as(C.c_void_p),
+                                          C.c_size_t(n), C.c_uint(max_iter), C.c_float(max_row_metric), C.c_float(beta),
+                                          post.ctypes.data_as(C.c_void_p), it.ctypes.data_as(C.c_void_p))
+        else:
+            self.lib.orc_decode_int8(C.byref(cs), llr.ctypes.data_as(C.c_void_p), C.c_size_t(n), C.c_uint(max_iter),
+                                     C.c_float(max_row_metric), C.c_float(beta), post.ctypes.data_as(C.c_void_p),
+                                     it.ctypes.data_as(C.c_void_p))
+        return post, it
+
+    def decode_f32(self, code, llr, mode=1, max_iter=10, max_row_metric=6e-8, beta=0.0):
+        llr = np.ascontiguousarray(llr, dtype=np.float32).reshape(-1, code.n)
+        n = llr.shape[0]
+        post = np.zeros_like(llr)
+        it = np.zeros(n, np.uint32)
+        cs, keep = self._code(code)
+        rc = self.lib.orc_decode_f32(C.byref(cs), C.byref(self._tree_struct()), C.c_int(mode),
+                                     llr.ctypes.data_as(C.c_void_p), C.c_size_t(n), C.c_uint(max_iter),
+                                     C.c_float(max_row_metric), C.c_float(beta), post.ctypes.data_as(C.c_void_p),
+                                     it.ctypes.data_as(C.c_void_p))
+        if rc != 0:
+            raise RuntimeError("orc_decode_f32 failed (row weight above the tree table)")
+        return post, it
+
+    def sigma(self, snr, llr_scale):
+        s, f = C.c_float(), C.c_float()
+        self.lib.orc_sigma(C.c_float(snr), C.c_float(llr_scale), C.byref(s), C.byref(f))
+        return s.value, f.value
+
+    def llr(self, bits, noise, snr, llr_scale, max_abs, punct=None, filler=None):
+        """Element-wise gen_metrics over flat arrays; returns (llr_f32, llr_i32, uncoded_errors)."""
+        sigma, sf = self.sigma(snr, llr_scale)
+        bits = np.asarray(bits, np.uint8).ravel()
+        noise = np.asarray(noise, np.float32).ravel()
+        pn = np.zeros(bits.size, np.uint8) if punct is None else np.asarray(punct, np.uint8).ravel()
+        fl = np.zeros(bits.size, np.uint8) if filler is None else np.asarray(filler, np.uint8).ravel()
+        lf = np.zeros(bits.size, np.float32)
+        li = np.zeros(bits.size, np.int32)
+        f = self.lib.orc_llr
+        f.restype = C.c_int
+        f.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, C.c_int,
+                      C.POINTER(C.c_float), C.POINTER(C.c_int32)]
+        errs = 0
+        pf = lf.ctypes.data_as(C.POINTER(C.c_float))
+        pi = li.ctypes.data_as(C.POINTER(C.c_int32))
+        for i in range(bits.size):
+            errs += f(int(bits[i]), float(noise[i]), sigma, sf, max_abs, int(pn[i]), int(fl[i]),
+                      C.cast(C.byref(pf.contents, 4 * i), C.POINTER(C.c_float)),
+                      C.cast(C.byref(pi.contents, 4 * i), C.POINTER(C.c_int32)))
+        return lf, li, errs
+
+    def encode(self, code, info):
+        info = np.ascontiguousarray(info, dtype=np.uint8).reshape(-1, (code.mcol - code.mrow) * code.z)
+        n = info.shape[0]
+        sched = []
+        recs = code.enc_schedule()
+        for pc, terms in recs:
+            sched += [pc, len(terms)]
+            for col, sh in terms:
+                sched += [col, sh]
+        sched = np.array(sched, np.int32)
+        cw = np.zeros((n, code.n), np.uint8)
+        self.lib.orc_encode(C.c_int(code.z), C.c_int(code.mcol), C.c_int(code.mrow), sched.ctypes.data_as(C.c_void_p),
+                            C.c_int(len(recs)), info.ctypes.data_as(C.c_void_p), C.c_size_t(n), cw.ctypes.data_as(C.c_void_p))
+        return cw
+
+    def count_errors(self, code, post, cw_bits):
+        post = np.ascontiguousarray(post)
+        cw_bits = np.ascontiguousarray(cw_bits, dtype=np.uint8)
+        n = post.shape[0]
+        a, b = C.c_uint64(), C.c_uint64()
+        fn = self.lib.orc_count_errors_i8 if post.dtype == np.int8 else self.lib.orc_count_errors_f32
+        if post.dtype not in (np.int8, np.float32):
+            raise TypeError(post.dtype)
+        fn(C.c_int(code.z), C.c_int(code.mcol), C.c_int(code.mrow), C.c_int(code.num_par),
+           post.ctypes.data_as(C.c_void_p), cw_bits.ctypes.data_as(C.c_void_p), C.c_size_t(n), C.byref(a), C.byref(b))
+        return a.value, b.value
