@@ -1,0 +1,201 @@
+/* ldpc_b200.h -- C ABI of the B200 QC-LDPC simulation engine.
+ *
+ * Drop-in boundary for the reference's hot path (tomt-1/simd-fecfun).  The
+ * reference exposes C++-linkage free functions with vectorclass types in
+ * their signatures (prototypes: src/Top/LDPCtop.cpp:26-39); this header
+ * replaces them with plain C types, opaque handles and status codes.
+ *
+ * Conventions
+ *   - Every call returns an int status (LDPC_OK = 0) and never exits the
+ *     process; ldpc_last_error() gives a message for the calling thread.
+ *   - "dev" pointers are CUDA device pointers, and the call is asynchronous on
+ *     `stream` (a cudaStream_t passed as void*; NULL = legacy default stream).
+ *     "_host" calls take host memory and return when the results are there.
+ *   - Codeword bit and LLR order is the reference's: column-major blocks,
+ *     element c*Z + t is bit t of base-matrix column c (N = Z*mcol elements).
+ *   - Hard decisions / data bits are packed LSB-first into 32-bit words:
+ *     bit i of a codeword (i < kbits = Z*(mcol-mrow)) is bit (i%32) of word
+ *     i/32; each codeword takes hard_words = ceil(kbits/32) words.
+ *   - A context is bound to one device and is not thread-safe; different
+ *     contexts are independent.
+ */
+#ifndef LDPC_B200_H
+#define LDPC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    LDPC_OK = 0,
+    LDPC_ERR_INVALID_ARG = 1,
+    LDPC_ERR_BAD_TABLE = 2,     /* malformed or truncated .dat table */
+    LDPC_ERR_UNSUPPORTED = 3,   /* parameters outside what the kernels implement */
+    LDPC_ERR_CUDA = 4,
+    LDPC_ERR_TIMEOUT = 5,       /* a bounded device wait gave up */
+    LDPC_ERR_IO = 6,
+    LDPC_ERR_NOMEM = 7
+};
+
+enum {
+    LDPC_INT8_OMS = 0,          /* int8 offset min-sum   (LDPCtop_Vec64c_min)  */
+    LDPC_F32_SP = 1,            /* float sum-product     (LDPCtop_Vec16f_prod) */
+    LDPC_F32_OMS = 2            /* float offset min-sum  (LDPCtop_Vec16f_min)  */
+};
+
+typedef struct ldpc_code ldpc_code;
+typedef struct ldpc_ctx ldpc_ctx;
+
+typedef struct {
+    int z, mrow, mcol;          /* lifting size and base-matrix shape */
+    int n;                      /* Z*mcol codeword bits */
+    int kbits;                  /* Z*(mcol-mrow) data bits (filler included) */
+    int num_par;                /* interleaved sub-codewords per codeword */
+    int fill_cnt;               /* filler bits */
+    int edges;                  /* Z * sum(row weights) */
+    int max_row_weight;
+    int hard_words;             /* ceil(kbits/32) */
+    int has_encoder;            /* encoder schedule present */
+} ldpc_code_info;
+
+/* Decoder configuration: the reference's run-time knobs
+ * (sim_struct_LDPC.h:3-20) plus the variant, which the reference selects at
+ * compile time (build/Makefile:9-14). */
+typedef struct {
+    int variant;                /* LDPC_INT8_OMS / LDPC_F32_SP / LDPC_F32_OMS */
+    unsigned max_iter;          /* maximum decoder iterations (1..255) */
+    float max_row_metric;       /* min-sum clamp, or 1-clamp for sum-product */
+    float beta;                 /* offset (truncated to an integer for int8) */
+    float llr_scale;            /* LLR_scaling_factor */
+    float max_abs_llr;          /* max_abs_LLR */
+} ldpc_cfg;
+
+/* Message for the most recent failure on the calling thread ("" if none). */
+const char *ldpc_last_error(void);
+
+/* Number of CUDA devices visible (0 when none; never an error). */
+int ldpc_device_count(int *count);
+
+/* ---- codes -------------------------------------------------------------- */
+
+/* Load the reference's two table files.  Replaces encode_matrix_allocate()
+ * (src/LDPCEnc/encode_matrix_allocate.cpp:38-92) and decode_matrix_allocate()
+ * (src/LDPCDec/decode_matrix_allocate.cpp:12-61); unlike those it checks
+ * every read and returns LDPC_ERR_IO / LDPC_ERR_BAD_TABLE instead of exiting.
+ * enc_path may be NULL (decoder only). */
+int ldpc_code_load_dat(const char *enc_path, const char *dec_path, ldpc_code **out);
+
+/* Same from in-memory images of the two files (int32 words, little endian). */
+int ldpc_code_from_tables(const int32_t *dec_words, size_t n_dec_words, const int32_t *enc_words,
+                          size_t n_enc_words, ldpc_code **out);
+
+int ldpc_code_get_info(const ldpc_code *code, ldpc_code_info *info);
+void ldpc_code_destroy(ldpc_code *code);
+
+/* ---- contexts ------------------------------------------------------------- */
+
+/* Binds a code and a configuration to a CUDA device and uploads the tables.
+ * Validates the configuration against the chosen variant. */
+int ldpc_ctx_create(const ldpc_code *code, const ldpc_cfg *cfg, int device, ldpc_ctx **out);
+void ldpc_ctx_destroy(ldpc_ctx *ctx);
+
+/* ---- decoding ------------------------------------------------------------- */
+
+/* Decode n codewords of int8 LLRs (variant LDPC_INT8_OMS).  Replaces
+ * LDPCdecode_set() (src/LDPCDec/LDPCdecode.cpp:203-245), which decodes in
+ * place and returns only the sum of iterations; here the results go to
+ * separate buffers, each optional (NULL = not wanted):
+ *   post_out  [n][N] int8 final posteriors (the reference's decoded_metrics)
+ *   hard_out  [n][hard_words] packed hard decisions of the data bits
+ *   iters_out [n] iterations each codeword ran (LDPCdecode's return value)
+ * dev pointers; asynchronous on stream. */
+int ldpc_decode_int8(ldpc_ctx *ctx, const int8_t *llr, size_t n, int8_t *post_out, uint32_t *hard_out,
+                     uint8_t *iters_out, void *stream);
+
+/* Float decoders (LDPC_F32_SP, LDPC_F32_OMS): same contract, float LLRs and
+ * posteriors. */
+int ldpc_decode_f32(ldpc_ctx *ctx, const float *llr, size_t n, float *post_out, uint32_t *hard_out,
+                    uint8_t *iters_out, void *stream);
+
+/* Host-memory versions: copy in, decode, copy out (chunked and overlapped);
+ * return when the outputs are in host memory.  *tot_iter (optional) receives
+ * the sum of iterations, LDPCdecode_set's return value. */
+int ldpc_decode_int8_host(ldpc_ctx *ctx, const int8_t *llr, size_t n, int8_t *post_out, uint32_t *hard_out,
+                          uint8_t *iters_out, uint64_t *tot_iter);
+int ldpc_decode_f32_host(ldpc_ctx *ctx, const float *llr, size_t n, float *post_out, uint32_t *hard_out,
+                         uint8_t *iters_out, uint64_t *tot_iter);
+
+/* Literal drop-in for LDPCdecode_set (LDPCdecode.cpp:203-245): decodes, in
+ * place, num_codeword codewords stored in the reference's padded host layout
+ * -- per codeword mcol columns of (ceil(Z/simd_par)+2)*simd_par elements,
+ * element t of column c at offset simd_par + t (decode_matrix_allocate.cpp:55)
+ * -- with int8 elements for LDPC_INT8_OMS and float for the float variants.
+ * *tot_iter receives the sum of iterations. */
+int ldpc_decode_set_compat(ldpc_ctx *ctx, void *decoded_metrics, unsigned num_codeword, unsigned simd_par,
+                           uint64_t *tot_iter);
+
+/* ---- channel generation -------------------------------------------------- */
+
+/* Fused generation: random data bits, QC encoding, BPSK, AWGN and LLR
+ * quantisation in one kernel.  Replaces gen_rand_databits()
+ * (src/Top/gen_rand_databits.cpp:11-40), LDPCencode()
+ * (src/LDPCEnc/LDPCencode.cpp:40-100), normdist2()
+ * (src/RNGfunc/prng_functions.cpp:148-186) and gen_metrics()
+ * (src/Top/gen_metrics.cpp:18-121).  Codeword i of SNR point s uses data and
+ * noise drawn from Philox4x32-10 keyed by `seed` at counter (cw_offset + i),
+ * so every SNR point sees the same data and the same noise, scaled by its
+ * sigma, as the reference's inner loop does (LDPCtop.cpp:89-97).
+ * Outputs (dev):
+ *   llr_i8 or llr_f32  [n_snr][n_per_snr][N]   (one of them, by variant)
+ *   data_bits          [n_per_snr][hard_words] sent data bits (optional)
+ *   uncoded_err        [n_snr] sign errors before decoding (optional,
+ *                      accumulated: caller zeroes)                         */
+int ldpc_generate(ldpc_ctx *ctx, uint64_t seed, uint64_t cw_offset, const float *snr_db, size_t n_snr,
+                  size_t n_per_snr, int8_t *llr_i8, float *llr_f32, uint32_t *data_bits,
+                  unsigned long long *uncoded_err, void *stream);
+
+/* LLR quantisation of given noise (dev): cw_bits [n][N] 0/1 bytes,
+ * noise [n][N] float -> llr [n][N] (int8 or float by variant) at one SNR.
+ * Bit-exact restatement of gen_metrics(); used for parity checks. */
+int ldpc_llr_from_noise(ldpc_ctx *ctx, const uint8_t *cw_bits, const float *noise, size_t n, float snr_db,
+                        int8_t *llr_i8, float *llr_f32, unsigned long long *uncoded_err, void *stream);
+
+/* QC encoding (dev): data_bits [n][hard_words] packed -> cw_bits [n][N]
+ * 0/1 bytes.  Replaces LDPCencode() (LDPCencode.cpp:40-100). */
+int ldpc_encode(ldpc_ctx *ctx, const uint32_t *data_bits, size_t n, uint8_t *cw_bits, void *stream);
+
+/* ---- simulation ------------------------------------------------------------ */
+
+/* Per-SNR counters of a simulation run, the reference's per-loop report
+ * (LDPCtop.cpp:127-129). */
+typedef struct {
+    float snr_db;
+    unsigned long long codewords;
+    unsigned long long iterations;
+    unsigned long long bit_errors;
+    unsigned long long cw_errors;       /* counted per sub-codeword, LDPC_count_errors.cpp:124-131 */
+    unsigned long long uncoded_errors;
+    double decode_ms;                   /* device time of the decode kernel */
+} ldpc_snr_stats;
+
+/* One outer-loop pass of the reference's simulator (LDPCtop.cpp:86-139) for
+ * n_per_snr codewords at each SNR: generate, decode, count errors, on the
+ * device.  Codeword counters start at cw_offset, so consecutive calls (or
+ * ranks of a multi-GPU run) with different offsets draw disjoint data. */
+int ldpc_simulate(ldpc_ctx *ctx, uint64_t seed, uint64_t cw_offset, const float *snr_db, size_t n_snr,
+                  size_t n_per_snr, ldpc_snr_stats *stats);
+
+/* Count errors of decoded hard decisions (dev): hard [n][hard_words] against
+ * sent data_bits [n % ref_period][hard_words], codeword errors per
+ * sub-codeword.  Replaces LDPC_count_errors() (LDPC_count_errors.cpp:40-136).
+ * Results accumulate into counters[0..1] = {cw_errors, bit_errors}. */
+int ldpc_count_errors(ldpc_ctx *ctx, const uint32_t *hard, size_t n, const uint32_t *data_bits, size_t ref_period,
+                      unsigned long long *counters, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LDPC_B200_H */

@@ -1,0 +1,126 @@
+// Host side of the int8 offset min-sum decoder: kernel selection, launch geometry, launch.
+#include <algorithm>
+#include <cstring>
+
+#include "internal.h"
+#include "oms_f16.cuh"
+
+namespace ldpc {
+
+namespace {
+// Shapes compiled with the check messages in registers.  Exact shapes first
+// (802.11ad rate 1/2: 8 layers of weights 5,6,6,6,7,7,7,8), then padded ones.
+using Shape11ad12 = FixedShape<5, 6, 6, 6, 7, 7, 7, 8>;
+const int kRw11ad12[] = {5, 6, 6, 6, 7, 7, 7, 8};
+#define OMS_FIXED(S_, RW_, T_) {S_::L, S_::D, RW_, oms_f16_kernel<S_, false, T_>, oms_f16_kernel<S_, true, T_>}
+#define OMS_PAD(L_, D_, T_) {L_, D_, nullptr, oms_f16_kernel<PaddedShape<L_, D_>, false, T_>, oms_f16_kernel<PaddedShape<L_, D_>, true, T_>}
+const OmsInst kOmsInst[] = {
+    OMS_FIXED(Shape11ad12, kRw11ad12, 640),
+    OMS_PAD(8, 8, 384), OMS_PAD(12, 8, 384), OMS_PAD(8, 12, 384), OMS_PAD(6, 16, 384),
+    OMS_PAD(4, 16, 384), OMS_PAD(3, 16, 384), OMS_PAD(4, 24, 384),
+};
+#undef OMS_FIXED
+#undef OMS_PAD
+
+bool matches(const OmsInst& in, const ldpc_code& c) {
+    if (in.L != c.mrow) return false;
+    if (in.rw) {
+        for (int l = 0; l < in.L; ++l)
+            if (in.rw[l] != c.row_weights[l]) return false;
+        return true;
+    }
+    return in.D >= c.max_row_weight;
+}
+}  // namespace
+
+int setup_oms(ldpc_ctx* x) {
+    const ldpc_code& c = x->code;
+    const int L = c.mrow;
+    const OmsInst* best = nullptr;
+    for (const OmsInst& in : kOmsInst) {
+        if (!matches(in, c)) continue;
+        if (in.rw) { best = &in; break; }
+        if (!best || in.D < best->D) best = &in;
+    }
+    if (!best)
+        return fail(LDPC_ERR_UNSUPPORTED, "int8 decoder: no kernel for %d layers of weight <= %d (Z=%d)", L,
+                    c.max_row_weight, c.z);
+    if (L > OMS_MAX_L || L * best->D > OMS_MAX_SLOTS_E)
+        return fail(LDPC_ERR_UNSUPPORTED, "int8 decoder: %d layers x %d edge slots exceed the parameter block", L, best->D);
+    x->inst = best;
+    OmsTables& t = x->omst;
+    memset(&t, 0, sizeof(t));
+    t.z = c.z;
+    t.mcol = c.mcol;
+    t.n = c.z * c.mcol;
+    t.L = L;
+    t.D = best->D;
+    t.kbits = x->kbits;
+    t.hard_words = x->hard_words;
+    int e0 = 0;
+    for (int l = 0; l < L; ++l) {
+        t.rw[l] = (int16_t)c.row_weights[l];
+        for (int j = 0; j < c.row_weights[l]; ++j) {
+            const int slot = best->rw ? e0 + j : l * best->D + j;   // FixedShape / PaddedShape::slot
+            t.colz[slot] = c.row_cols[e0 + j] * c.z;
+            t.shift[slot] = (int16_t)c.row_shifts[e0 + j];
+        }
+        e0 += c.row_weights[l];
+    }
+    oms_fn k = x->beta0 ? best->k_beta0 : best->k_beta;
+    cudaFuncAttributes fa;
+    CUDA_TRY(cudaFuncGetAttributes(&fa, (const void*)k));
+    // groups per CTA: as many as the thread limit allows, at most 16 (2 slots each)
+    int G = std::min(16, fa.maxThreadsPerBlock / c.z);
+    if (G < 1) return fail(LDPC_ERR_UNSUPPORTED, "int8 decoder: Z=%d too large for the register kernel", c.z);
+    // shared memory: G groups of `stride` words; stride = n rounded so that
+    // stride mod 32 = ceil(32/G) (consecutive groups start in different banks)
+    const int spread = (32 + G - 1) / G;
+    const int stride = t.n + (((spread - t.n) % 32) + 32) % 32;
+    t.G = G;
+    t.stride = stride;
+    x->oms_threads = ((G * c.z + 31) / 32) * 32;
+    x->oms_smem = G * stride * 4;
+    CUDA_TRY(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, x->oms_smem));
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k, x->oms_threads, x->oms_smem));
+    if (per_sm < 1)
+        return fail(LDPC_ERR_UNSUPPORTED, "int8 decoder: %d threads x %d B shared memory do not fit an SM",
+                    x->oms_threads, x->oms_smem);
+    x->oms_ctas = per_sm * x->sms;
+    return LDPC_OK;
+}
+
+int launch_oms(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s) {
+    if (!x->inst) return fail(LDPC_ERR_INVALID_ARG, "context was not created for the int8 decoder");
+    if (a.n == 0) return LDPC_OK;
+    if (a.queue < 0 || a.queue >= ldpc_ctx::kQueues) return fail(LDPC_ERR_INVALID_ARG, "queue %d", a.queue);
+    OmsJob job;
+    memset(&job, 0, sizeof(job));
+    job.llr = (const int8_t*)a.llr;
+    job.ncw = (long long)a.n;
+    job.post_out = (int8_t*)a.post;
+    job.hard_out = a.hard;
+    job.iters_out = a.iters;
+    job.ref_bits = a.ref_bits;
+    job.ref_period = a.ref_period > 0 ? a.ref_period : 1;
+    job.bucket_size = a.bucket_size > 0 ? a.bucket_size : (long long)a.n;
+    job.counters = a.counters;
+    job.n_buckets = std::max(1, std::min(a.n_buckets, OMS_MAX_BUCKETS));
+    job.num_par = x->code.num_par;
+    job.max_iter = (int)x->cfg.max_iter;
+    job.beta2 = x->beta2;
+    job.maxv2 = x->maxv2;
+    job.queue = x->d_queue + a.queue;
+    job.status = x->d_status;
+    CUDA_TRY(cudaMemsetAsync(job.queue, 0, sizeof(unsigned long long), s));
+    const long long slots = 2LL * x->omst.G;
+    const long long want = ((long long)a.n + slots - 1) / slots;
+    const int grid = (int)std::min<long long>(want, x->oms_ctas);
+    oms_fn k = x->beta0 ? x->inst->k_beta0 : x->inst->k_beta;
+    k<<<grid, x->oms_threads, x->oms_smem, s>>>(x->omst, job);
+    CUDA_TRY(cudaGetLastError());
+    return LDPC_OK;
+}
+
+}  // namespace ldpc

@@ -1,0 +1,98 @@
+// Internal declarations shared by the translation units of libldpc_b200.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "ldpc_b200.h"
+#include "tables.h"
+
+namespace ldpc {
+
+int fail(int code, const char* fmt, ...);
+
+#define CUDA_TRY(expr)                                                                                    \
+    do {                                                                                                  \
+        cudaError_t e_ = (expr);                                                                          \
+        if (e_ != cudaSuccess) return ::ldpc::fail(LDPC_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
+    } while (0)
+
+typedef void (*oms_fn)(const OmsTables, const OmsJob);
+typedef void (*sp_fn)(const SpTables, const SpJob);
+
+struct OmsInst {
+    int L, D;            // layers, edge slots per layer (padded shapes)
+    const int* rw;       // exact row weights (fixed shapes) or nullptr
+    oms_fn k_beta, k_beta0;
+};
+
+// Arguments of one decode launch (device pointers).
+struct DecodeArgs {
+    const void* llr = nullptr;
+    size_t n = 0;
+    void* post = nullptr;
+    uint32_t* hard = nullptr;
+    uint8_t* iters = nullptr;
+    const uint32_t* ref_bits = nullptr;
+    long long ref_period = 1;
+    long long bucket_size = 0;
+    unsigned long long* counters = nullptr;
+    int n_buckets = 0;
+    int queue = 0;
+};
+
+}  // namespace ldpc
+
+struct ldpc_code {
+    int z = 0, mrow = 0, mcol = 0, max_row_weight = 0;
+    std::vector<int32_t> row_weights, row_cols, row_shifts;
+    bool has_enc = false;
+    int num_par = 1;
+    std::vector<int32_t> par_cnts, par_colnum, par_offset, punc_list, fill_list;
+    int fill_cnt = 0;
+    // decoded encoder schedule: parity record i computes column sched_col[i] as the XOR of
+    // columns term_col[k] rotated by term_shift[k], k in [sched_first[i], +sched_cnt[i])
+    std::vector<int32_t> sched_col, sched_first, sched_cnt, term_col, term_shift;
+    std::vector<uint8_t> punct, filler;   // [n] 0/1 masks
+};
+
+struct ldpc_ctx {
+    ldpc_code code;
+    ldpc_cfg cfg;
+    int device = 0;
+    int sms = 0;
+    int n = 0, kbits = 0, hard_words = 0;
+    // int8 offset min-sum
+    const ldpc::OmsInst* inst = nullptr;
+    ldpc::OmsTables omst;
+    int oms_threads = 0, oms_smem = 0, oms_ctas = 0;
+    uint32_t beta2 = 0, maxv2 = 0;
+    bool beta0 = false;
+    // float decoders
+    ldpc::SpTables spt;
+    ldpc::sp_fn sp_kernel = nullptr;
+    int sp_threads = 0, sp_smem = 0, sp_ctas = 0;
+    float maxf = 0.f;
+    // generation
+    ldpc::GenTables gent;
+    uint8_t* d_masks = nullptr;                 // punct[n] then filler[n]
+    // device scratch
+    static constexpr int kQueues = 4;
+    unsigned long long* d_queue = nullptr;      // work counters, one per concurrent launch
+    unsigned int* d_status = nullptr;
+    unsigned long long* d_counters = nullptr;   // [OMS_MAX_BUCKETS][4] decode counters + [OMS_MAX_BUCKETS] uncoded
+    cudaStream_t streams[2] = {nullptr, nullptr};
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+};
+
+namespace ldpc {
+int setup_oms(ldpc_ctx* x);
+int launch_oms(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s);
+int setup_sp(ldpc_ctx* x);
+int launch_sp(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s);
+int setup_gen(ldpc_ctx* x);
+void release_gen(ldpc_ctx* x);
+uint32_t half2_bits(float v);
+}  // namespace ldpc

@@ -1,0 +1,106 @@
+// Kernel parameter blocks shared by the host code and the kernels.
+#pragma once
+#include <stdint.h>
+
+namespace ldpc {
+
+constexpr int OMS_MAX_L = 48;
+constexpr int OMS_MAX_SLOTS_E = 256;   // L*D edge slots carried in the kernel parameters
+constexpr int OMS_MAX_BUCKETS = 32;
+
+struct OmsTables {
+    int z, mcol, n, stride, G;
+    int L, D;
+    int kbits;                       // data columns * Z (hard-decision bits per codeword)
+    int hard_words;                  // ceil(kbits / 32)
+    int16_t rw[OMS_MAX_L];
+    int32_t colz[OMS_MAX_SLOTS_E];   // column * Z of edge slot l*D + j
+    int16_t shift[OMS_MAX_SLOTS_E];  // circulant shift of edge slot l*D + j
+};
+
+struct OmsJob {
+    const int8_t* llr;               // [ncw][n]
+    long long ncw;
+    int8_t* post_out;                // [ncw][n] or null
+    uint32_t* hard_out;              // [ncw][hard_words] or null; bit i of codeword = data bit i, LSB first
+    uint8_t* iters_out;              // [ncw] or null
+    const uint32_t* ref_bits;        // [ref_period][hard_words] sent data bits, or null
+    long long ref_period;
+    long long bucket_size;           // codewords per counter bucket (e.g. per SNR point)
+    unsigned long long* counters;    // [n_buckets][4]: codewords, iterations, bit errors, codeword errors
+    int n_buckets;
+    int num_par;                     // interleaved sub-codewords per codeword (codeword errors counted per slot t % num_par)
+    int max_iter;
+    uint32_t beta2;                  // half2 bits of beta8
+    uint32_t maxv2;                  // half2 bits of Max8
+    unsigned long long* queue;       // work counter, zero before launch
+    unsigned int* status;            // error word (0 = ok)
+};
+
+// ---- float decoders (sum-product / offset min-sum), R in shared memory ----
+constexpr int SP_MAX_L = 64;
+constexpr int SP_MAX_E = 512;
+
+struct SpTables {
+    int z, mcol, n, L, G;            // G = codewords per CTA (one per lane group of Z threads)
+    int kbits, hard_words;
+    int E;                           // sum of row weights
+    int16_t rw[SP_MAX_L];
+    int16_t ebase[SP_MAX_L];         // first edge of layer l
+    int32_t colz[SP_MAX_E];          // column * Z of edge e
+    int16_t shift[SP_MAX_E];
+};
+
+struct SpJob {
+    const float* llr;
+    long long ncw;
+    float* post_out;
+    uint32_t* hard_out;
+    uint8_t* iters_out;
+    const uint32_t* ref_bits;
+    long long ref_period;
+    long long bucket_size;
+    unsigned long long* counters;
+    int n_buckets;
+    int num_par;
+    int max_iter;
+    int prod;                        // 1 = sum-product, 0 = offset min-sum
+    float beta;
+    float maxv;                      // Max_val as decode_row computes it
+    unsigned long long* queue;
+};
+
+// ---- fused generation ----
+constexpr int GEN_MAX_TERMS = 1024;
+constexpr int GEN_MAX_PAR = 64;
+constexpr int GEN_MAX_COLS = 128;
+constexpr int GEN_MAX_SNR = 32;
+
+struct GenTables {
+    int z, mcol, mrow, n, kbits, hard_words, words_per_col;
+    int n_par;                       // parity records in schedule order
+    int16_t par_col[GEN_MAX_PAR];
+    int16_t par_first[GEN_MAX_PAR];
+    int16_t par_cnt[GEN_MAX_PAR];
+    int16_t term_col[GEN_MAX_TERMS];
+    int16_t term_shift[GEN_MAX_TERMS];
+    const uint8_t* punct;            // [n] 0/1, device
+    const uint8_t* filler;           // [n] 0/1, device
+    int any_punct, any_filler;
+};
+
+struct GenJob {
+    uint64_t seed;
+    uint64_t cw_offset;
+    long long n_per_snr;
+    int n_snr;
+    float sigma[GEN_MAX_SNR];
+    float sigma_factor[GEN_MAX_SNR];
+    float max_abs;
+    int8_t* llr_i8;                  // [n_snr][n_per_snr][n] or null
+    float* llr_f32;                  // [n_snr][n_per_snr][n] or null
+    uint32_t* data_bits;             // [n_per_snr][hard_words] or null
+    unsigned long long* uncoded;     // [n_snr] or null
+};
+
+}  // namespace ldpc
