@@ -120,6 +120,17 @@ int ldpc_decode_int8(ldpc_ctx *ctx, const int8_t *llr, size_t n, int8_t *post_ou
 int ldpc_decode_f32(ldpc_ctx *ctx, const float *llr, size_t n, float *post_out, uint32_t *hard_out,
                     uint8_t *iters_out, void *stream);
 
+/* Decode with fused error counting (either variant; dev pointers, async).
+ * Codeword i is compared with sent data bits data_bits[i % ref_period] and
+ * counted in bucket min(i / bucket_size, n_buckets-1) of
+ * counters[n_buckets][4] = {codewords, iterations, bit errors, codeword
+ * errors per sub-codeword} (LDPC_count_errors.cpp:40-136 fused into the
+ * decoder's write-out); counters accumulate, the caller zeroes them.
+ * hard_out / iters_out are optional as in ldpc_decode_int8. */
+int ldpc_decode_count(ldpc_ctx *ctx, const void *llr, size_t n, uint32_t *hard_out, uint8_t *iters_out,
+                      const uint32_t *data_bits, size_t ref_period, size_t bucket_size, unsigned long long *counters,
+                      int n_buckets, void *stream);
+
 /* Host-memory versions: copy in, decode, copy out (chunked and overlapped);
  * return when the outputs are in host memory.  *tot_iter (optional) receives
  * the sum of iterations, LDPCdecode_set's return value. */
@@ -194,6 +205,14 @@ int ldpc_simulate(ldpc_ctx *ctx, uint64_t seed, uint64_t cw_offset, const float 
  * Results accumulate into counters[0..1] = {cw_errors, bit_errors}. */
 int ldpc_count_errors(ldpc_ctx *ctx, const uint32_t *hard, size_t n, const uint32_t *data_bits, size_t ref_period,
                       unsigned long long *counters, void *stream);
+
+/* ---- measurement ----------------------------------------------------------- */
+
+/* Sustained 32-bit integer instruction rate of `device` (ops/s), from a
+ * microbenchmark of independent lop3 / iadd chains: the peak against which
+ * the decoder's integer-pipe roofline fraction is reported.  No counterpart
+ * in the reference (which times with RDTSC only, LDPCtop.cpp:107-114). */
+int ldpc_probe_int32_peak(int device, double *ops_per_s);
 
 #ifdef __cplusplus
 }

@@ -295,3 +295,19 @@ void orc_count_errors_f32(int z, int mcol, int mrow, int num_par, const float *p
     }
     free(hard);
 }
+
+int64_t orc_llr_array(const uint8_t *bits, const float *noise, size_t total, int n, const uint8_t *punct,
+                      const uint8_t *filler, float snr, float llr_scale, float max_abs, float *llr_f, int8_t *llr_i8) {
+    float sigma, sf;
+    int64_t errs = 0;
+    orc_sigma(snr, llr_scale, &sigma, &sf);
+    for (size_t e = 0; e < total; ++e) {
+        const int idx = (int)(e % (size_t)n);
+        float l;
+        int32_t li;
+        errs += orc_llr(bits[e] & 1, noise[e], sigma, sf, max_abs, punct ? punct[idx] : 0, filler ? filler[idx] : 0, &l, &li);
+        if (llr_f) llr_f[e] = l;
+        if (llr_i8) llr_i8[e] = (int8_t)(int16_t)li;
+    }
+    return errs;
+}

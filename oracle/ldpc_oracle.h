@@ -57,6 +57,11 @@ void orc_sigma(float snr, float llr_scale, float *sigma, float *sigma_factor);
 int orc_llr(int bit, float noise, float sigma, float sigma_factor, float max_abs, int punct,
             int filler, float *llr_f, int32_t *llr_i);
 
+/* orc_llr over [total] elements of codewords of n bits (masks indexed by
+ * element % n, may be NULL); returns the uncoded error count */
+int64_t orc_llr_array(const uint8_t *bits, const float *noise, size_t total, int n, const uint8_t *punct,
+                      const uint8_t *filler, float snr, float llr_scale, float max_abs, float *llr_f, int8_t *llr_i8);
+
 /* encode: info [n][K_cols*z] bits (0/1) -> cw [n][mcol*z] bits;
  * sched = (parity col, n terms, (col, shift) * n) records, n_par records */
 void orc_encode(int z, int mcol, int mrow, const int32_t *sched, int n_par, const uint8_t *info,

@@ -254,6 +254,25 @@ class Oracle:
                       C.cast(C.byref(pi.contents, 4 * i), C.POINTER(C.c_int32)))
         return lf, li, errs
 
+    def llr_array(self, code, bits, noise, snr, llr_scale, max_abs):
+        """gen_metrics over [n][N] bits and noise: (float LLRs, int8 LLRs, uncoded errors)."""
+        bits = np.ascontiguousarray(bits, dtype=np.uint8)
+        noise = np.ascontiguousarray(noise, dtype=np.float32)
+        lf = np.empty(bits.shape, np.float32)
+        li = np.empty(bits.shape, np.int8)
+        f = self.lib.orc_llr_array
+        f.restype = C.c_int64
+        pn = np.zeros(code.n, np.uint8)
+        fl = np.zeros(code.n, np.uint8)
+        for s, e in zip(code.punc_list[0::2], code.punc_list[1::2]):
+            pn[s:e + 1] ^= 1
+        for s, e in zip(code.fill_list[0::2], code.fill_list[1::2]):
+            fl[s:e + 1] ^= 1
+        errs = f(bits.ctypes.data_as(C.c_void_p), noise.ctypes.data_as(C.c_void_p), C.c_size_t(bits.size),
+                 C.c_int(code.n), pn.ctypes.data_as(C.c_void_p), fl.ctypes.data_as(C.c_void_p), C.c_float(snr),
+                 C.c_float(llr_scale), C.c_float(max_abs), lf.ctypes.data_as(C.c_void_p), li.ctypes.data_as(C.c_void_p))
+        return lf, li, int(errs)
+
     def encode(self, code, info):
         info = np.ascontiguousarray(info, dtype=np.uint8).reshape(-1, (code.mcol - code.mrow) * code.z)
         n = info.shape[0]

@@ -34,20 +34,18 @@ template <int BYTES> struct Raw {
     unsigned char b[BYTES];
 };
 
+/* Boolean vector as a bit mask (lane i = bit i), like AVX-512 mask registers. */
 template <int N> struct VecB {
-    bool m[N];
+    static_assert(N <= 64, "boolean vectors up to 64 lanes");
+    uint64_t bits;
+    static constexpr uint64_t all() { return N == 64 ? ~0ull : ((1ull << N) - 1); }
     VecB() = default;
-    void load_bits(uint64_t bits) {
-        for (int i = 0; i < N; ++i) m[i] = (bits >> i) & 1;
-    }
-    friend uint64_t to_bits(const VecB& v) {
-        uint64_t r = 0;
-        for (int i = 0; i < N; ++i) r |= (uint64_t)v.m[i] << i;
-        return r;
-    }
-    friend VecB operator&(const VecB& a, const VecB& b) { VecB r; for (int i = 0; i < N; ++i) r.m[i] = a.m[i] && b.m[i]; return r; }
-    friend VecB operator|(const VecB& a, const VecB& b) { VecB r; for (int i = 0; i < N; ++i) r.m[i] = a.m[i] || b.m[i]; return r; }
-    friend VecB operator~(const VecB& a) { VecB r; for (int i = 0; i < N; ++i) r.m[i] = !a.m[i]; return r; }
+    void load_bits(uint64_t b) { bits = b & all(); }
+    bool get(int i) const { return (bits >> i) & 1; }
+    friend uint64_t to_bits(const VecB& v) { return v.bits; }
+    friend VecB operator&(const VecB& a, const VecB& b) { VecB r; r.bits = a.bits & b.bits; return r; }
+    friend VecB operator|(const VecB& a, const VecB& b) { VecB r; r.bits = a.bits | b.bits; return r; }
+    friend VecB operator~(const VecB& a) { VecB r; r.bits = ~a.bits & all(); return r; }
 };
 
 template <class T> struct sat_lim {
@@ -62,7 +60,13 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
     T e[N];
 
     Vec() = default;
-    Vec(T v) { for (int i = 0; i < N; ++i) e[i] = v; }
+    Vec(T v) {
+#if defined(__AVX512BW__)
+        if constexpr (std::is_same<T, int8_t>::value && N == 64) { _mm512_storeu_si512(e, _mm512_set1_epi8(v)); return; }
+        if constexpr (std::is_same<T, float>::value && N == 16) { _mm512_storeu_ps(e, _mm512_set1_ps(v)); return; }
+#endif
+        for (int i = 0; i < N; ++i) e[i] = v;
+    }
     Vec(const Raw<BYTES>& r) { memcpy(e, r.b, BYTES); }
     template <class U, int M, class = typename std::enable_if<(int)sizeof(U) * M == BYTES && !(std::is_same<U, T>::value && M == N)>::type>
     explicit Vec(const Vec<U, M>& o) { memcpy(e, o.e, BYTES); }
@@ -132,6 +136,10 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
     /* ---- arithmetic ---- */
     friend Vec operator+(const Vec& a, const Vec& b) {
         Vec r;
+#if defined(__AVX512BW__)
+        if constexpr (std::is_same<T, int8_t>::value && N == 64) { _mm512_storeu_si512(r.e, _mm512_add_epi8(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r; }
+        if constexpr (std::is_same<T, float>::value && N == 16) { _mm512_storeu_ps(r.e, _mm512_add_ps(_mm512_loadu_ps(a.e), _mm512_loadu_ps(b.e))); return r; }
+#endif
         if constexpr (std::is_integral<T>::value) {
             using U = typename std::make_unsigned<T>::type;
             for (int i = 0; i < N; ++i) r.e[i] = (T)(U)((U)a.e[i] + (U)b.e[i]);
@@ -142,6 +150,10 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
     }
     friend Vec operator-(const Vec& a, const Vec& b) {
         Vec r;
+#if defined(__AVX512BW__)
+        if constexpr (std::is_same<T, int8_t>::value && N == 64) { _mm512_storeu_si512(r.e, _mm512_sub_epi8(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r; }
+        if constexpr (std::is_same<T, float>::value && N == 16) { _mm512_storeu_ps(r.e, _mm512_sub_ps(_mm512_loadu_ps(a.e), _mm512_loadu_ps(b.e))); return r; }
+#endif
         if constexpr (std::is_integral<T>::value) {
             using U = typename std::make_unsigned<T>::type;
             for (int i = 0; i < N; ++i) r.e[i] = (T)(U)((U)a.e[i] - (U)b.e[i]);
@@ -181,32 +193,53 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
     }
 
     /* ---- comparisons ---- */
-    friend VecB<N> operator<(const Vec& a, const Vec& b) {
-        VecB<N> r;
-#if defined(__AVX512BW__)
-        if constexpr (std::is_same<T, int8_t>::value && N == 64) {
-            uint64_t m = _mm512_cmplt_epi8_mask(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e));
-            r.load_bits(m); return r;
-        }
-#endif
-        for (int i = 0; i < N; ++i) r.m[i] = a.e[i] < b.e[i];
+    template <class F> static VecB<N> cmp(const Vec& a, const Vec& b, F f) {
+        VecB<N> r; r.bits = 0;
+        for (int i = 0; i < N; ++i) r.bits |= (uint64_t)(f(a.e[i], b.e[i]) ? 1 : 0) << i;
         return r;
     }
+#if defined(__AVX512BW__) && defined(__AVX512VL__)
+    template <int P> static bool cmp_fast(const Vec& a, const Vec& b, VecB<N>& r) {
+        if constexpr (std::is_same<T, int8_t>::value && N == 64) { r.bits = _mm512_cmp_epi8_mask(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e), P); return true; }
+        if constexpr (std::is_same<T, int16_t>::value && N == 32) { r.bits = _mm512_cmp_epi16_mask(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e), P); return true; }
+        if constexpr (std::is_same<T, int32_t>::value && N == 16) { r.bits = _mm512_cmp_epi32_mask(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e), P); return true; }
+        if constexpr (std::is_same<T, int32_t>::value && N == 8) { r.bits = _mm256_cmp_epi32_mask(_mm256_loadu_si256((const __m256i*)a.e), _mm256_loadu_si256((const __m256i*)b.e), P); return true; }
+        return false;
+    }
+#endif
+    friend VecB<N> operator<(const Vec& a, const Vec& b) {
+#if defined(__AVX512BW__) && defined(__AVX512VL__)
+        { VecB<N> r; if (cmp_fast<_MM_CMPINT_LT>(a, b, r)) return r; }
+        if constexpr (std::is_same<T, float>::value && N == 16) { VecB<N> r; r.bits = _mm512_cmp_ps_mask(_mm512_loadu_ps(a.e), _mm512_loadu_ps(b.e), _CMP_LT_OQ); return r; }
+        if constexpr (std::is_same<T, float>::value && N == 8) { VecB<N> r; r.bits = _mm256_cmp_ps_mask(_mm256_loadu_ps(a.e), _mm256_loadu_ps(b.e), _CMP_LT_OQ); return r; }
+#endif
+        return cmp(a, b, [](T x, T y) { return x < y; });
+    }
     friend VecB<N> operator>(const Vec& a, const Vec& b) { return b < a; }
-    friend VecB<N> operator<=(const Vec& a, const Vec& b) { VecB<N> r; for (int i = 0; i < N; ++i) r.m[i] = a.e[i] <= b.e[i]; return r; }
+    friend VecB<N> operator<=(const Vec& a, const Vec& b) { return cmp(a, b, [](T x, T y) { return x <= y; }); }
     friend VecB<N> operator>=(const Vec& a, const Vec& b) { return b <= a; }
-    friend VecB<N> operator==(const Vec& a, const Vec& b) { VecB<N> r; for (int i = 0; i < N; ++i) r.m[i] = a.e[i] == b.e[i]; return r; }
-    friend VecB<N> operator!=(const Vec& a, const Vec& b) { VecB<N> r; for (int i = 0; i < N; ++i) r.m[i] = a.e[i] != b.e[i]; return r; }
+    friend VecB<N> operator==(const Vec& a, const Vec& b) {
+#if defined(__AVX512BW__) && defined(__AVX512VL__)
+        { VecB<N> r; if (cmp_fast<_MM_CMPINT_EQ>(a, b, r)) return r; }
+#endif
+        return cmp(a, b, [](T x, T y) { return x == y; });
+    }
+    friend VecB<N> operator!=(const Vec& a, const Vec& b) { return cmp(a, b, [](T x, T y) { return x != y; }); }
 
     /* ---- element functions ---- */
     friend Vec select(const VecB<N>& s, const Vec& a, const Vec& b) {
 #if defined(__AVX512BW__)
         if constexpr (std::is_same<T, int8_t>::value && N == 64) {
-            Vec r; _mm512_storeu_si512(r.e, _mm512_mask_blend_epi8((__mmask64)to_bits(s), _mm512_loadu_si512(b.e), _mm512_loadu_si512(a.e)));
+            Vec r; _mm512_storeu_si512(r.e, _mm512_mask_blend_epi8((__mmask64)s.bits, _mm512_loadu_si512(b.e), _mm512_loadu_si512(a.e)));
             return r;
         }
 #endif
-        Vec r; for (int i = 0; i < N; ++i) r.e[i] = s.m[i] ? a.e[i] : b.e[i]; return r;
+#if defined(__AVX512BW__) && defined(__AVX512VL__)
+        if constexpr (BYTES == 64 && sizeof(T) == 2) { Vec r; _mm512_storeu_si512(r.e, _mm512_mask_blend_epi16((__mmask32)s.bits, _mm512_loadu_si512(b.e), _mm512_loadu_si512(a.e))); return r; }
+        if constexpr (BYTES == 64 && sizeof(T) == 4) { Vec r; _mm512_storeu_si512(r.e, _mm512_mask_blend_epi32((__mmask16)s.bits, _mm512_loadu_si512(b.e), _mm512_loadu_si512(a.e))); return r; }
+        if constexpr (BYTES == 32 && sizeof(T) == 4) { Vec r; _mm256_storeu_si256((__m256i*)r.e, _mm256_mask_blend_epi32((__mmask8)s.bits, _mm256_loadu_si256((const __m256i*)b.e), _mm256_loadu_si256((const __m256i*)a.e))); return r; }
+#endif
+        Vec r; for (int i = 0; i < N; ++i) r.e[i] = s.get(i) ? a.e[i] : b.e[i]; return r;
     }
     friend Vec if_sub(const VecB<N>& s, const Vec& a, const Vec& b) { return select(s, a - b, a); }
     friend Vec if_add(const VecB<N>& s, const Vec& a, const Vec& b) { return select(s, a + b, a); }

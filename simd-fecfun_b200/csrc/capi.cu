@@ -315,8 +315,10 @@ void ldpc_ctx_destroy(ldpc_ctx* x) {
     cudaFree(x->d_queue);
     cudaFree(x->d_status);
     cudaFree(x->d_counters);
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < 2; ++i) {
         if (x->streams[i]) cudaStreamDestroy(x->streams[i]);
+        for (int k = 0; k < 4; ++k) cudaFree(x->d_pipe[i][k]);
+    }
     if (x->ev_start) cudaEventDestroy(x->ev_start);
     if (x->ev_stop) cudaEventDestroy(x->ev_stop);
     ldpc::release_gen(x);
@@ -326,16 +328,6 @@ void ldpc_ctx_destroy(ldpc_ctx* x) {
 }  // extern "C"
 
 namespace {
-
-bool is_device_ptr(const void* p) {
-    if (!p) return true;
-    cudaPointerAttributes at;
-    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
-}
 
 int check_decode_args(ldpc_ctx* x, size_t n, const void* llr, int want_variant_int8) {
     if (!x) return fail(LDPC_ERR_INVALID_ARG, "ctx is NULL");
@@ -351,50 +343,65 @@ int check_decode_args(ldpc_ctx* x, size_t n, const void* llr, int want_variant_i
 // Host-buffer decoding: chunks alternate between two streams; each chunk is
 // copied in, decoded and copied out on its stream, so copies of one chunk
 // overlap the decode of the other.
+int pipe_buffer(ldpc_ctx* x, int b, int k, size_t bytes, void** out) {
+    if (bytes == 0) {
+        *out = nullptr;
+        return LDPC_OK;
+    }
+    if (x->pipe_bytes[b][k] < bytes) {
+        cudaFree(x->d_pipe[b][k]);
+        x->d_pipe[b][k] = nullptr;
+        x->pipe_bytes[b][k] = 0;
+        if (cudaMalloc(&x->d_pipe[b][k], bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(LDPC_ERR_NOMEM, "device buffer of %zu bytes", bytes);
+        }
+        x->pipe_bytes[b][k] = bytes;
+    }
+    *out = x->d_pipe[b][k];
+    return LDPC_OK;
+}
+
+// Host-buffer decoding: chunks alternate between two streams; each chunk is
+// copied in, decoded and copied out on its stream, so the copies of one chunk
+// overlap the decoding of the other.  Device buffers persist in the context.
 template <class T>
 int decode_host(ldpc_ctx* x, const T* llr, size_t n, T* post, uint32_t* hard, uint8_t* iters, uint64_t* tot_iter) {
     CUDA_TRY(cudaSetDevice(x->device));
     const size_t N = (size_t)x->n, HW = (size_t)x->hard_words;
     const size_t chunk = std::max<size_t>(1, std::min<size_t>(n, ((size_t)64 << 20) / (N * sizeof(T))));
-    T* d_llr[2] = {nullptr, nullptr};
-    T* d_post[2] = {nullptr, nullptr};
-    uint32_t* d_hard[2] = {nullptr, nullptr};
-    uint8_t* d_it[2] = {nullptr, nullptr};
-    int rc = LDPC_OK;
     std::vector<uint8_t> it_local;
     if (tot_iter && !iters) {
         it_local.resize(n);
         iters = it_local.data();
     }
-    for (int b = 0; b < 2; ++b) {
-        if (cudaMalloc(&d_llr[b], chunk * N * sizeof(T)) != cudaSuccess ||
-            (post && cudaMalloc(&d_post[b], chunk * N * sizeof(T)) != cudaSuccess) ||
-            (hard && cudaMalloc(&d_hard[b], chunk * HW * 4) != cudaSuccess) ||
-            (iters && cudaMalloc(&d_it[b], chunk) != cudaSuccess)) {
-            rc = fail(LDPC_ERR_NOMEM, "device buffers for a %zu-codeword chunk", chunk);
-            break;
-        }
-    }
+    int rc = LDPC_OK;
     for (size_t off = 0, ci = 0; rc == LDPC_OK && off < n; off += chunk, ++ci) {
         const int b = (int)(ci & 1);
         cudaStream_t s = x->streams[b];
         const size_t m = std::min(chunk, n - off);
-        if (cudaMemcpyAsync(d_llr[b], llr + off * N, m * N * sizeof(T), cudaMemcpyHostToDevice, s) != cudaSuccess) {
+        void *d_llr, *d_post, *d_hard, *d_it;
+        if ((rc = pipe_buffer(x, b, 0, chunk * N * sizeof(T), &d_llr)) ||
+            (rc = pipe_buffer(x, b, 1, post ? chunk * N * sizeof(T) : 0, &d_post)) ||
+            (rc = pipe_buffer(x, b, 2, hard ? chunk * HW * 4 : 0, &d_hard)) ||
+            (rc = pipe_buffer(x, b, 3, iters ? chunk : 0, &d_it)))
+            break;
+        if (cudaMemcpyAsync(d_llr, llr + off * N, m * N * sizeof(T), cudaMemcpyHostToDevice, s) != cudaSuccess) {
             rc = fail(LDPC_ERR_CUDA, "copy-in: %s", cudaGetErrorString(cudaGetLastError()));
             break;
         }
         ldpc::DecodeArgs a;
-        a.llr = d_llr[b];
+        a.llr = d_llr;
         a.n = m;
-        a.post = d_post[b];
-        a.hard = d_hard[b];
-        a.iters = d_it[b];
+        a.post = d_post;
+        a.hard = (uint32_t*)d_hard;
+        a.iters = (uint8_t*)d_it;
         a.queue = b;
         rc = (x->cfg.variant == LDPC_INT8_OMS) ? ldpc::launch_oms(x, a, s) : ldpc::launch_sp(x, a, s);
         if (rc) break;
-        if ((post && cudaMemcpyAsync(post + off * N, d_post[b], m * N * sizeof(T), cudaMemcpyDeviceToHost, s)) ||
-            (hard && cudaMemcpyAsync(hard + off * HW, d_hard[b], m * HW * 4, cudaMemcpyDeviceToHost, s)) ||
-            (iters && cudaMemcpyAsync(iters + off, d_it[b], m, cudaMemcpyDeviceToHost, s))) {
+        if ((post && cudaMemcpyAsync(post + off * N, d_post, m * N * sizeof(T), cudaMemcpyDeviceToHost, s)) ||
+            (hard && cudaMemcpyAsync(hard + off * HW, d_hard, m * HW * 4, cudaMemcpyDeviceToHost, s)) ||
+            (iters && cudaMemcpyAsync(iters + off, d_it, m, cudaMemcpyDeviceToHost, s))) {
             rc = fail(LDPC_ERR_CUDA, "copy-out: %s", cudaGetErrorString(cudaGetLastError()));
             break;
         }
@@ -402,12 +409,6 @@ int decode_host(ldpc_ctx* x, const T* llr, size_t n, T* post, uint32_t* hard, ui
     for (int b = 0; b < 2; ++b) {
         cudaError_t e = cudaStreamSynchronize(x->streams[b]);
         if (e != cudaSuccess && rc == LDPC_OK) rc = fail(LDPC_ERR_CUDA, "decode: %s", cudaGetErrorString(e));
-    }
-    for (int b = 0; b < 2; ++b) {
-        cudaFree(d_llr[b]);
-        cudaFree(d_post[b]);
-        cudaFree(d_hard[b]);
-        cudaFree(d_it[b]);
     }
     if (rc == LDPC_OK && tot_iter) {
         uint64_t s = 0;
@@ -447,6 +448,29 @@ int ldpc_decode_f32(ldpc_ctx* x, const float* llr, size_t n, float* post_out, ui
     a.hard = hard_out;
     a.iters = iters_out;
     return ldpc::launch_sp(x, a, (cudaStream_t)stream);
+}
+
+int ldpc_decode_count(ldpc_ctx* x, const void* llr, size_t n, uint32_t* hard_out, uint8_t* iters_out,
+                      const uint32_t* data_bits, size_t ref_period, size_t bucket_size, unsigned long long* counters,
+                      int n_buckets, void* stream) {
+    if (!x) return fail(LDPC_ERR_INVALID_ARG, "ctx is NULL");
+    if (n && !llr) return fail(LDPC_ERR_INVALID_ARG, "llr is NULL");
+    if (counters && (!data_bits || ref_period == 0 || n_buckets < 1 || n_buckets > ldpc::OMS_MAX_BUCKETS))
+        return fail(LDPC_ERR_INVALID_ARG, "counting needs data_bits, ref_period > 0 and 1..%d buckets",
+                    ldpc::OMS_MAX_BUCKETS);
+    CUDA_TRY(cudaSetDevice(x->device));
+    ldpc::DecodeArgs a;
+    a.llr = llr;
+    a.n = n;
+    a.hard = hard_out;
+    a.iters = iters_out;
+    a.ref_bits = counters ? data_bits : nullptr;
+    a.ref_period = (long long)ref_period;
+    a.bucket_size = bucket_size ? (long long)bucket_size : (long long)n;
+    a.counters = counters;
+    a.n_buckets = n_buckets;
+    return x->cfg.variant == LDPC_INT8_OMS ? ldpc::launch_oms(x, a, (cudaStream_t)stream)
+                                           : ldpc::launch_sp(x, a, (cudaStream_t)stream);
 }
 
 int ldpc_decode_int8_host(ldpc_ctx* x, const int8_t* llr, size_t n, int8_t* post_out, uint32_t* hard_out,

@@ -1,6 +1,227 @@
-// Fused generation (filled in with the Philox/encode/LLR kernel).
+// Host side of channel generation, encoding, error counting and the
+// simulation driver (ldpc_generate / ldpc_encode / ldpc_llr_from_noise /
+// ldpc_count_errors / ldpc_simulate).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "gen.cuh"
 #include "internal.h"
+
 namespace ldpc {
-int setup_gen(ldpc_ctx* x) { (void)x; return LDPC_OK; }
-void release_gen(ldpc_ctx* x) { (void)x; }
+
+namespace {
+// gen_metrics.cpp:26-30, evaluated with the same float/double steps
+void sigma_of(float snr, float llr_scale, float* sigma, float* sf) {
+    const float three_db = 10 * log10f(2.0f);
+    const float s = powf(10.0f, (float)((double)(snr + three_db) / -20.0));
+    *sigma = s;
+    *sf = 2 * llr_scale / (s * s);
+}
+
+int gen_grid(ldpc_ctx* x, long long n, int* smem) {
+    const GenTables& t = x->gent;
+    *smem = gen_warp_words(t.kbits, t.mcol, t.z, t.n) * 4 * 8;
+    const long long want = (n + 7) / 8;
+    return (int)std::max<long long>(1, std::min<long long>(want, (long long)x->sms * 8));
+}
+}  // namespace
+
+int setup_gen(ldpc_ctx* x) {
+    const ldpc_code& c = x->code;
+    GenTables& t = x->gent;
+    memset(&t, 0, sizeof(t));
+    if (c.mrow > GEN_MAX_PAR || (int)c.term_col.size() > GEN_MAX_TERMS || c.mcol > GEN_MAX_COLS)
+        return fail(LDPC_ERR_UNSUPPORTED, "encoder schedule too large (%d parity columns, %zu terms)", c.mrow,
+                    c.term_col.size());
+    t.z = c.z;
+    t.mcol = c.mcol;
+    t.mrow = c.mrow;
+    t.n = c.z * c.mcol;
+    t.kbits = x->kbits;
+    t.hard_words = x->hard_words;
+    t.words_per_col = (c.z + 31) / 32;
+    t.n_par = c.mrow;
+    for (int i = 0; i < c.mrow; ++i) {
+        t.par_col[i] = (int16_t)c.sched_col[i];
+        t.par_first[i] = (int16_t)c.sched_first[i];
+        t.par_cnt[i] = (int16_t)c.sched_cnt[i];
+    }
+    for (size_t k = 0; k < c.term_col.size(); ++k) {
+        t.term_col[k] = (int16_t)c.term_col[k];
+        t.term_shift[k] = (int16_t)c.term_shift[k];
+    }
+    t.any_punct = std::any_of(c.punct.begin(), c.punct.end(), [](uint8_t v) { return v != 0; });
+    t.any_filler = std::any_of(c.filler.begin(), c.filler.end(), [](uint8_t v) { return v != 0; });
+    CUDA_TRY(cudaMalloc(&x->d_masks, 2 * (size_t)t.n));
+    CUDA_TRY(cudaMemcpy(x->d_masks, c.punct.data(), t.n, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(x->d_masks + t.n, c.filler.data(), t.n, cudaMemcpyHostToDevice));
+    t.punct = x->d_masks;
+    t.filler = x->d_masks + t.n;
+    int smem = 0;
+    gen_grid(x, 1, &smem);
+    if (smem > 200 * 1024) return fail(LDPC_ERR_UNSUPPORTED, "generator needs %d B of shared memory", smem);
+    CUDA_TRY(cudaFuncSetAttribute((const void*)gen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(cudaFuncSetAttribute((const void*)encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return LDPC_OK;
+}
+
+void release_gen(ldpc_ctx* x) {
+    cudaFree(x->d_masks);
+    x->d_masks = nullptr;
+    cudaFree(x->d_sim_llr);
+    cudaFree(x->d_sim_data);
+    cudaFree(x->d_sim_hard);
+    x->d_sim_llr = nullptr;
+    x->d_sim_data = nullptr;
+    x->d_sim_hard = nullptr;
+}
+
+int launch_gen(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* snr_db, size_t n_snr, size_t n_per_snr,
+               int8_t* llr_i8, float* llr_f32, uint32_t* data_bits, unsigned long long* uncoded, cudaStream_t s) {
+    if (!x->code.has_enc) return fail(LDPC_ERR_INVALID_ARG, "code has no encoder table");
+    if (n_snr < 1 || n_snr > (size_t)GEN_MAX_SNR) return fail(LDPC_ERR_INVALID_ARG, "n_snr=%zu outside 1..%d", n_snr, GEN_MAX_SNR);
+    if (!snr_db) return fail(LDPC_ERR_INVALID_ARG, "snr_db is NULL");
+    if (n_per_snr == 0) return LDPC_OK;
+    GenJob job;
+    memset(&job, 0, sizeof(job));
+    job.seed = seed;
+    job.cw_offset = cw_offset;
+    job.n_per_snr = (long long)n_per_snr;
+    job.n_snr = (int)n_snr;
+    for (size_t i = 0; i < n_snr; ++i) sigma_of(snr_db[i], x->cfg.llr_scale, &job.sigma[i], &job.sigma_factor[i]);
+    job.max_abs = x->cfg.max_abs_llr;
+    job.llr_i8 = llr_i8;
+    job.llr_f32 = llr_f32;
+    job.data_bits = data_bits;
+    job.uncoded = uncoded;
+    int smem = 0;
+    const int grid = gen_grid(x, (long long)n_per_snr, &smem);
+    gen_kernel<<<grid, 256, smem, s>>>(x->gent, job);
+    CUDA_TRY(cudaGetLastError());
+    return LDPC_OK;
+}
+
 }  // namespace ldpc
+
+using ldpc::fail;
+
+extern "C" {
+
+int ldpc_generate(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* snr_db, size_t n_snr, size_t n_per_snr,
+                  int8_t* llr_i8, float* llr_f32, uint32_t* data_bits, unsigned long long* uncoded, void* stream) {
+    if (!x) return fail(LDPC_ERR_INVALID_ARG, "ctx is NULL");
+    CUDA_TRY(cudaSetDevice(x->device));
+    return ldpc::launch_gen(x, seed, cw_offset, snr_db, n_snr, n_per_snr, llr_i8, llr_f32, data_bits, uncoded,
+                            (cudaStream_t)stream);
+}
+
+int ldpc_encode(ldpc_ctx* x, const uint32_t* data_bits, size_t n, uint8_t* cw_bits, void* stream) {
+    if (!x) return fail(LDPC_ERR_INVALID_ARG, "ctx is NULL");
+    if (!x->code.has_enc) return fail(LDPC_ERR_INVALID_ARG, "code has no encoder table");
+    if (n == 0) return LDPC_OK;
+    if (!data_bits || !cw_bits) return fail(LDPC_ERR_INVALID_ARG, "NULL buffer");
+    CUDA_TRY(cudaSetDevice(x->device));
+    int smem = 0;
+    const int grid = ldpc::gen_grid(x, (long long)n, &smem);
+    ldpc::encode_kernel<<<grid, 256, smem, (cudaStream_t)stream>>>(x->gent, data_bits, (long long)n, cw_bits);
+    CUDA_TRY(cudaGetLastError());
+    return LDPC_OK;
+}
+
+int ldpc_llr_from_noise(ldpc_ctx* x, const uint8_t* cw_bits, const float* noise, size_t n, float snr_db, int8_t* llr_i8,
+                        float* llr_f32, unsigned long long* uncoded, void* stream) {
+    if (!x) return fail(LDPC_ERR_INVALID_ARG, "ctx is NULL");
+    if (!x->code.has_enc) return fail(LDPC_ERR_INVALID_ARG, "code has no encoder table (puncture/filler masks)");
+    if (n == 0) return LDPC_OK;
+    if (!cw_bits || !noise || (!llr_i8 && !llr_f32)) return fail(LDPC_ERR_INVALID_ARG, "NULL buffer");
+    CUDA_TRY(cudaSetDevice(x->device));
+    float sigma, sf;
+    ldpc::sigma_of(snr_db, x->cfg.llr_scale, &sigma, &sf);
+    const long long total = (long long)n * x->n;
+    const int grid = (int)std::min<long long>((total + 255) / 256, (long long)x->sms * 16);
+    ldpc::llr_from_noise_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(x->gent, cw_bits, noise, total, sigma, sf,
+                                                                       x->cfg.max_abs_llr, llr_i8, llr_f32, uncoded);
+    CUDA_TRY(cudaGetLastError());
+    return LDPC_OK;
+}
+
+int ldpc_count_errors(ldpc_ctx* x, const uint32_t* hard, size_t n, const uint32_t* data_bits, size_t ref_period,
+                      unsigned long long* counters, void* stream) {
+    if (!x) return fail(LDPC_ERR_INVALID_ARG, "ctx is NULL");
+    if (n == 0) return LDPC_OK;
+    if (!hard || !data_bits || !counters || ref_period == 0) return fail(LDPC_ERR_INVALID_ARG, "NULL buffer or period");
+    CUDA_TRY(cudaSetDevice(x->device));
+    const int grid = (int)std::min<long long>(((long long)n + 7) / 8, (long long)x->sms * 8);
+    ldpc::count_errors_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(hard, (long long)n, data_bits,
+                                                                      (long long)ref_period, x->hard_words, x->kbits,
+                                                                      x->code.z, x->code.num_par, counters);
+    CUDA_TRY(cudaGetLastError());
+    return LDPC_OK;
+}
+
+int ldpc_simulate(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* snr_db, size_t n_snr, size_t n_per_snr,
+                  ldpc_snr_stats* stats) {
+    if (!x || !snr_db || !stats) return fail(LDPC_ERR_INVALID_ARG, "NULL argument");
+    if (n_snr < 1 || n_snr > (size_t)ldpc::GEN_MAX_SNR) return fail(LDPC_ERR_INVALID_ARG, "n_snr=%zu", n_snr);
+    CUDA_TRY(cudaSetDevice(x->device));
+    const bool is8 = x->cfg.variant == LDPC_INT8_OMS;
+    const size_t N = (size_t)x->n, es = is8 ? 1 : 4;
+    // chunk so that the LLRs of all SNR points fit in ~2 GB
+    size_t chunk = std::max<size_t>(1, std::min<size_t>(n_per_snr, ((size_t)2 << 30) / (n_snr * N * es)));
+    if (x->sim_cap < chunk * n_snr) {
+        cudaFree(x->d_sim_llr);
+        cudaFree(x->d_sim_data);
+        cudaFree(x->d_sim_hard);
+        x->d_sim_llr = x->d_sim_data = x->d_sim_hard = nullptr;
+        x->sim_cap = 0;
+        CUDA_TRY(cudaMalloc(&x->d_sim_llr, chunk * n_snr * N * es));
+        CUDA_TRY(cudaMalloc(&x->d_sim_data, chunk * x->hard_words * 4));
+        x->sim_cap = chunk * n_snr;
+    }
+    cudaStream_t s = x->streams[0];
+    unsigned long long* dc = x->d_counters;   // [n_snr][4] decode + [n_snr] uncoded
+    CUDA_TRY(cudaMemsetAsync(dc, 0, sizeof(unsigned long long) * ldpc::OMS_MAX_BUCKETS * 5, s));
+    std::vector<double> ms(n_snr, 0.0);
+    for (size_t off = 0; off < n_per_snr; off += chunk) {
+        const size_t m = std::min(chunk, n_per_snr - off);
+        int rc = ldpc::launch_gen(x, seed, cw_offset + off, snr_db, n_snr, m, is8 ? (int8_t*)x->d_sim_llr : nullptr,
+                                  is8 ? nullptr : (float*)x->d_sim_llr, (uint32_t*)x->d_sim_data,
+                                  dc + ldpc::OMS_MAX_BUCKETS * 4, s);
+        if (rc) return rc;
+        for (size_t k = 0; k < n_snr; ++k) {
+            ldpc::DecodeArgs a;
+            a.llr = (const uint8_t*)x->d_sim_llr + k * m * N * es;
+            a.n = m;
+            a.ref_bits = (const uint32_t*)x->d_sim_data;
+            a.ref_period = (long long)m;
+            a.bucket_size = (long long)m;
+            a.counters = dc + 4 * k;
+            a.n_buckets = 1;
+            CUDA_TRY(cudaEventRecord(x->ev_start, s));
+            rc = is8 ? ldpc::launch_oms(x, a, s) : ldpc::launch_sp(x, a, s);
+            if (rc) return rc;
+            CUDA_TRY(cudaEventRecord(x->ev_stop, s));
+            CUDA_TRY(cudaEventSynchronize(x->ev_stop));
+            float t = 0.f;
+            CUDA_TRY(cudaEventElapsedTime(&t, x->ev_start, x->ev_stop));
+            ms[k] += t;
+        }
+    }
+    std::vector<unsigned long long> h(ldpc::OMS_MAX_BUCKETS * 5);
+    CUDA_TRY(cudaMemcpyAsync(h.data(), dc, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    for (size_t k = 0; k < n_snr; ++k) {
+        stats[k].snr_db = snr_db[k];
+        stats[k].codewords = h[4 * k + 0];
+        stats[k].iterations = h[4 * k + 1];
+        stats[k].bit_errors = h[4 * k + 2];
+        stats[k].cw_errors = h[4 * k + 3];
+        stats[k].uncoded_errors = h[ldpc::OMS_MAX_BUCKETS * 4 + k];
+        stats[k].decode_ms = ms[k];
+    }
+    return LDPC_OK;
+}
+
+}  // extern "C"

@@ -78,12 +78,19 @@ struct ldpc_ctx {
     // generation
     ldpc::GenTables gent;
     uint8_t* d_masks = nullptr;                 // punct[n] then filler[n]
+    void* d_sim_llr = nullptr;                  // ldpc_simulate scratch: LLRs of one chunk, all SNR points
+    void* d_sim_data = nullptr;                 //   sent data bits of the chunk
+    void* d_sim_hard = nullptr;
+    size_t sim_cap = 0;                         //   codewords the LLR scratch holds
     // device scratch
     static constexpr int kQueues = 4;
     unsigned long long* d_queue = nullptr;      // work counters, one per concurrent launch
     unsigned int* d_status = nullptr;
     unsigned long long* d_counters = nullptr;   // [OMS_MAX_BUCKETS][4] decode counters + [OMS_MAX_BUCKETS] uncoded
     cudaStream_t streams[2] = {nullptr, nullptr};
+    // host-buffer pipeline: per stream, device buffers for one chunk (grow-only)
+    void* d_pipe[2][4] = {{nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}};
+    size_t pipe_bytes[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
 };
 
@@ -93,6 +100,8 @@ int launch_oms(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s);
 int setup_sp(ldpc_ctx* x);
 int launch_sp(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s);
 int setup_gen(ldpc_ctx* x);
+int launch_gen(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* snr_db, size_t n_snr, size_t n_per_snr,
+               int8_t* llr_i8, float* llr_f32, uint32_t* data_bits, unsigned long long* uncoded, cudaStream_t s);
 void release_gen(ldpc_ctx* x);
 uint32_t half2_bits(float v);
 }  // namespace ldpc

@@ -75,6 +75,8 @@ _PROTOS = {
     "ldpc_encode": (C.c_int, [_vp, _vp, _sz, _vp, _vp]),
     "ldpc_simulate": (C.c_int, [_vp, C.c_uint64, C.c_uint64, _vp, _sz, _sz, C.POINTER(SnrStats)]),
     "ldpc_count_errors": (C.c_int, [_vp, _vp, _sz, _vp, _sz, _vp, _vp]),
+    "ldpc_decode_count": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _sz, _sz, _vp, C.c_int, _vp]),
+    "ldpc_probe_int32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
 }
 
 if not os.path.exists(LIB_PATH):
@@ -100,6 +102,12 @@ def device_count() -> int:
     n = C.c_int()
     check(lib.ldpc_device_count(C.byref(n)))
     return n.value
+
+
+def probe_int32_peak(device: int = 0) -> float:
+    v = C.c_double()
+    check(lib.ldpc_probe_int32_peak(device, C.byref(v)))
+    return v.value
 
 
 def _ptr(x) -> Optional[int]:
@@ -185,6 +193,11 @@ class Context:
 
     def decode_f32(self, llr, n, post=None, hard=None, iters=None, stream=0):
         check(lib.ldpc_decode_f32(self.h, _ptr(llr), n, _ptr(post), _ptr(hard), _ptr(iters), stream or None))
+
+    def decode_count(self, llr, n, hard=None, iters=None, data_bits=None, ref_period=1, bucket_size=0, counters=None,
+                     n_buckets=1, stream=0):
+        check(lib.ldpc_decode_count(self.h, _ptr(llr), n, _ptr(hard), _ptr(iters), _ptr(data_bits), ref_period,
+                                    bucket_size, _ptr(counters), n_buckets, stream or None))
 
     def generate(self, seed, cw_offset, snr_db, n_per_snr, llr_i8=None, llr_f32=None, data_bits=None, uncoded=None,
                  stream=0):
