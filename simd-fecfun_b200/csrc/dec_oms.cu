@@ -1,8 +1,10 @@
 // Host side of the int8 offset min-sum decoder: kernel selection, launch geometry, launch.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 #include "internal.h"
+#include "codes_fixed.cuh"
 #include "oms_f16.cuh"
 
 namespace ldpc {
@@ -12,14 +14,39 @@ namespace {
 // (802.11ad rate 1/2: 8 layers of weights 5,6,6,6,7,7,7,8), then padded ones.
 using Shape11ad12 = FixedShape<5, 6, 6, 6, 7, 7, 7, 8>;
 const int kRw11ad12[] = {5, 6, 6, 6, 7, 7, 7, 8};
-#define OMS_FIXED(S_, RW_, T_) {S_::L, S_::D, RW_, oms_f16_kernel<S_, false, T_>, oms_f16_kernel<S_, true, T_>}
-#define OMS_PAD(L_, D_, T_) {L_, D_, nullptr, oms_f16_kernel<PaddedShape<L_, D_>, false, T_>, oms_f16_kernel<PaddedShape<L_, D_>, true, T_>}
+#define OMS_K(S_, T_, B_) {T_, B_, oms_f16_kernel<S_, false, T_, B_>, oms_f16_kernel<S_, true, T_, B_>}
+#define OMS_FIXED(S_, RW_) {S_::L, S_::D, RW_, nullptr, 0, 4, {OMS_K(S_, 640, 1), OMS_K(S_, 256, 2), OMS_K(S_, 192, 3), OMS_K(S_, 128, 5)}}
+#define OMS_COMPILED(C_, RW_) {C_::L, C_::D, RW_, &kCompiled##C_, 0, 4, {OMS_K(CompiledShape<C_>, 640, 1), OMS_K(CompiledShape<C_>, 256, 2), OMS_K(CompiledShape<C_>, 192, 3), OMS_K(CompiledShape<C_>, 128, 5)}}
+#define OMS_SPLIT(C_, RW_, EREG_)                                                                           \
+    {C_::L, C_::D, RW_, &kCompiled##C_, C_::E - EREG_, 2,                                                    \
+     {{128, 7, oms_f16_kernel<SplitShape<C_, EREG_>, false, 128, 7>, oms_f16_kernel<SplitShape<C_, EREG_>, true, 128, 7>}, \
+      {96, 8, oms_f16_kernel<SplitShape<C_, EREG_>, false, 96, 8>, oms_f16_kernel<SplitShape<C_, EREG_>, true, 96, 8>}}}
+#define OMS_PAD(L_, D_) {L_, D_, nullptr, nullptr, 0, 1, {{384, 1, oms_f16_kernel<PaddedShape<L_, D_>, false, 384, 1>, oms_f16_kernel<PaddedShape<L_, D_>, true, 384, 1>}}}
+// compiled-in code descriptions (columns, shifts) for table matching
+template <class C>
+CompiledCode describe() {
+    CompiledCode d;
+    d.z = C::Z;
+    d.L = C::L;
+    d.E = C::E;
+    for (int e = 0; e < C::E; ++e) {
+        d.col[e] = C::col(e);
+        d.shift[e] = C::shift(e);
+    }
+    return d;
+}
+const CompiledCode kCompiledCode11ad12 = describe<Code11ad12>();
+
 const OmsInst kOmsInst[] = {
-    OMS_FIXED(Shape11ad12, kRw11ad12, 640),
-    OMS_PAD(8, 8, 384), OMS_PAD(12, 8, 384), OMS_PAD(8, 12, 384), OMS_PAD(6, 16, 384),
-    OMS_PAD(4, 16, 384), OMS_PAD(3, 16, 384), OMS_PAD(4, 24, 384),
+    OMS_SPLIT(Code11ad12, kRw11ad12, 30),
+    OMS_COMPILED(Code11ad12, kRw11ad12),
+    OMS_FIXED(Shape11ad12, kRw11ad12),
+    OMS_PAD(8, 8), OMS_PAD(12, 8), OMS_PAD(8, 12), OMS_PAD(6, 16), OMS_PAD(4, 16), OMS_PAD(3, 16), OMS_PAD(4, 24),
 };
+#undef OMS_K
 #undef OMS_FIXED
+#undef OMS_COMPILED
+#undef OMS_SPLIT
 #undef OMS_PAD
 
 bool matches(const OmsInst& in, const ldpc_code& c) {
@@ -27,6 +54,21 @@ bool matches(const OmsInst& in, const ldpc_code& c) {
     if (in.rw) {
         for (int l = 0; l < in.L; ++l)
             if (in.rw[l] != c.row_weights[l]) return false;
+        if (in.compiled) {
+            // same columns; each layer's shifts = compiled shifts + one constant (mod Z)
+            const CompiledCode& k = *in.compiled;
+            if (k.z != c.z) return false;
+            int e0 = 0;
+            for (int l = 0; l < in.L; ++l) {
+                const int d = c.row_weights[l];
+                const int rot = ((c.row_shifts[e0] - k.shift[e0]) % c.z + c.z) % c.z;
+                for (int j = 0; j < d; ++j) {
+                    if (c.row_cols[e0 + j] != k.col[e0 + j]) return false;
+                    if (((k.shift[e0 + j] + rot) % c.z) != c.row_shifts[e0 + j]) return false;
+                }
+                e0 += d;
+            }
+        }
         return true;
     }
     return in.D >= c.max_row_weight;
@@ -37,8 +79,10 @@ int setup_oms(ldpc_ctx* x) {
     const ldpc_code& c = x->code;
     const int L = c.mrow;
     const OmsInst* best = nullptr;
+    const bool use_compiled = !getenv("LDPC_OMS_NO_COMPILED");
+    const bool use_split = !getenv("LDPC_OMS_NO_SPLIT");
     for (const OmsInst& in : kOmsInst) {
-        if (!matches(in, c)) continue;
+        if (!matches(in, c) || (in.compiled && !use_compiled) || (in.smem_edges && !use_split)) continue;
         if (in.rw) { best = &in; break; }
         if (!best || in.D < best->D) best = &in;
     }
@@ -67,12 +111,31 @@ int setup_oms(ldpc_ctx* x) {
         }
         e0 += c.row_weights[l];
     }
-    oms_fn k = x->beta0 ? best->k_beta0 : best->k_beta;
-    cudaFuncAttributes fa;
-    CUDA_TRY(cudaFuncGetAttributes(&fa, (const void*)k));
-    // groups per CTA: as many as the thread limit allows, at most 16 (2 slots each)
-    int G = std::min(16, fa.maxThreadsPerBlock / c.z);
+    // groups per CTA: LDPC_OMS_G forces it (tuning); else the most groups the
+    // widest compiled launch allows (<= 16: two slots per group, 32 slots)
+    int G = 0;
+    if (const char* e = getenv("LDPC_OMS_G")) G = atoi(e);
+    const OmsLaunch* lv = nullptr;
+    if (G > 0) {
+        for (int i = 0; i < best->n_launch; ++i) {
+            const OmsLaunch& cand = best->launch[i];
+            if (((G * c.z + 31) / 32) * 32 <= cand.max_threads && (!lv || cand.max_threads < lv->max_threads)) lv = &cand;
+        }
+        if (!lv || G > 16) return fail(LDPC_ERR_UNSUPPORTED, "int8 decoder: %d groups of Z=%d do not fit a compiled launch", G, c.z);
+    } else {
+        // default: the launch whose CTA is closest to 128 threads (small CTAs keep
+        // the per-layer barriers cheap; the autotuner may choose differently)
+        for (int i = 0; i < best->n_launch; ++i) {
+            const OmsLaunch& cand = best->launch[i];
+            if (cand.max_threads < c.z) continue;
+            if (!lv || std::abs(cand.max_threads - 128) < std::abs(lv->max_threads - 128)) lv = &cand;
+        }
+        if (!lv) lv = &best->launch[0];
+        G = std::min(16, lv->max_threads / c.z);
+    }
     if (G < 1) return fail(LDPC_ERR_UNSUPPORTED, "int8 decoder: Z=%d too large for the register kernel", c.z);
+    x->oms_launch = lv;
+    oms_fn k = x->beta0 ? lv->k_beta0 : lv->k_beta;
     // shared memory: G groups of `stride` words; stride = n rounded so that
     // stride mod 32 = ceil(32/G) (consecutive groups start in different banks)
     const int spread = (32 + G - 1) / G;
@@ -80,7 +143,9 @@ int setup_oms(ldpc_ctx* x) {
     t.G = G;
     t.stride = stride;
     x->oms_threads = ((G * c.z + 31) / 32) * 32;
-    x->oms_smem = G * stride * 4;
+    x->oms_threads = ((G * c.z + 31) / 32) * 32;
+    // posteriors + LLR staging + shared-memory check messages
+    x->oms_smem = ((G * stride * 4 + 15) & ~15) + 2 * G * ((t.n + 15) & ~15) + best->smem_edges * x->oms_threads * 4;
     CUDA_TRY(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, x->oms_smem));
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k, x->oms_threads, x->oms_smem));
@@ -113,11 +178,10 @@ int launch_oms(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s) {
     job.maxv2 = x->maxv2;
     job.queue = x->d_queue + a.queue;
     job.status = x->d_status;
-    CUDA_TRY(cudaMemsetAsync(job.queue, 0, sizeof(unsigned long long), s));
     const long long slots = 2LL * x->omst.G;
     const long long want = ((long long)a.n + slots - 1) / slots;
     const int grid = (int)std::min<long long>(want, x->oms_ctas);
-    oms_fn k = x->beta0 ? x->inst->k_beta0 : x->inst->k_beta;
+    oms_fn k = x->beta0 ? x->oms_launch->k_beta0 : x->oms_launch->k_beta;
     k<<<grid, x->oms_threads, x->oms_smem, s>>>(x->omst, job);
     CUDA_TRY(cudaGetLastError());
     return LDPC_OK;

@@ -22,10 +22,23 @@ int fail(int code, const char* fmt, ...);
 typedef void (*oms_fn)(const OmsTables, const OmsJob);
 typedef void (*sp_fn)(const SpTables, const SpJob);
 
+struct OmsLaunch {
+    int max_threads, min_blocks;   // __launch_bounds__ of this compilation
+    oms_fn k_beta, k_beta0;
+};
+
+struct CompiledCode {
+    int z, L, E;
+    int col[256], shift[256];
+};
+
 struct OmsInst {
     int L, D;            // layers, edge slots per layer (padded shapes)
     const int* rw;       // exact row weights (fixed shapes) or nullptr
-    oms_fn k_beta, k_beta0;
+    const CompiledCode* compiled;   // code compiled in completely, or nullptr
+    int smem_edges;                 // edge slots whose messages live in shared memory
+    int n_launch;
+    OmsLaunch launch[4];
 };
 
 // Arguments of one decode launch (device pointers).
@@ -66,6 +79,7 @@ struct ldpc_ctx {
     int n = 0, kbits = 0, hard_words = 0;
     // int8 offset min-sum
     const ldpc::OmsInst* inst = nullptr;
+    const ldpc::OmsLaunch* oms_launch = nullptr;
     ldpc::OmsTables omst;
     int oms_threads = 0, oms_smem = 0, oms_ctas = 0;
     uint32_t beta2 = 0, maxv2 = 0;

@@ -40,20 +40,35 @@
 
 #include <utility>
 
+#include "codes_fixed.cuh"
 #include "tables.h"
 
 namespace ldpc {
 
-__device__ __forceinline__ uint32_t h2u(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
-__device__ __forceinline__ __half2 u2h(uint32_t u) { return *reinterpret_cast<__half2*>(&u); }
+// Packed half2 operations on 32-bit registers (inline PTX keeps the two
+// lanes in one register; no split into 16-bit halves).
+__device__ __forceinline__ uint32_t hsub2(uint32_t a, uint32_t b) { uint32_t d; asm("sub.rn.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); return d; }
+__device__ __forceinline__ uint32_t hadd2(uint32_t a, uint32_t b) { uint32_t d; asm("add.rn.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); return d; }
+__device__ __forceinline__ uint32_t hmin2(uint32_t a, uint32_t b) { uint32_t d; asm("min.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); return d; }
+__device__ __forceinline__ uint32_t hmax2(uint32_t a, uint32_t b) { uint32_t d; asm("max.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); return d; }
+__device__ __forceinline__ uint32_t hfma2(uint32_t a, uint32_t b, uint32_t c) { uint32_t d; asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c)); return d; }
+// 0xffff in each lane where a == b, else 0
+__device__ __forceinline__ uint32_t heq2_mask(uint32_t a, uint32_t b) { uint32_t d; asm("set.eq.u32.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); return d; }
+// 1.0 in each lane where a == b, else 0.0
+__device__ __forceinline__ uint32_t heq2(uint32_t a, uint32_t b) { uint32_t d; asm("set.eq.f16x2.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); return d; }
+__device__ __forceinline__ uint32_t habs2(uint32_t a) { return a & 0x7fff7fffu; }
+
+constexpr uint32_t H2_M128 = 0xd800d800u;   // -128.0 in both lanes
+constexpr uint32_t H2_P127 = 0x57f057f0u;   // +127.0
+constexpr uint32_t H2_ZERO = 0u;
+constexpr uint32_t H2_1024 = 0x64006400u;   // 1024.0
 
 template <bool BETA0>
-__device__ __forceinline__ __half2 abs_q(__half2 q) {
-    __half2 a = __habs2(q);
+__device__ __forceinline__ uint32_t abs_q(uint32_t q) {
+    uint32_t a = habs2(q);
     if (BETA0) {
         // abs8(-128) = -128, and max(-128 - 0, 0) = 0: that edge contributes m = 0
-        __half2 is128 = __heq2(q, __float2half2_rn(-128.0f));
-        a = __hfma2(is128, __float2half2_rn(-128.0f), a);
+        a = hfma2(heq2(q, H2_M128), H2_M128, a);
     }
     return a;
 }
@@ -63,10 +78,17 @@ __device__ __forceinline__ __half2 abs_q(__half2 q) {
 //   FixedShape<rw...>: exact row weights; edge e of layer l is rw[0]+..+rw[l-1]+j.
 //   PaddedShape<L,D>: L layers of at most D edges; the weights come from the
 //                     tables at run time, edge slot = l*D + j.
+// Column-local position (t + s) mod z of check t's edge with shift s, with
+// t < z and s < z: min over unsigned of (t + s) and (t + s - z).
+__device__ __forceinline__ int wrap_add(int t, int s, int z) {
+    return (int)min((unsigned)(t + s), (unsigned)(t + s - z));
+}
+
 template <int... RW>
 struct FixedShape {
     static constexpr int L = sizeof...(RW);
     static constexpr int E = (RW + ...);
+    static constexpr int E_REG = E;
     static constexpr int D = [] { int m = 0; for (int v : {RW...}) m = v > m ? v : m; return m; }();
     __host__ __device__ static constexpr int maxd(int l) {
         constexpr int rw[] = {RW...};
@@ -79,7 +101,35 @@ struct FixedShape {
         return b + j;
     }
     __device__ static bool has(const OmsTables&, int, int) { return true; }
+    // shared-memory word of edge e for check row t of a group starting at gbase
+    __device__ static int addr(const OmsTables& tb, int e, int t, int gbase) {
+        return gbase + tb.colz[e] + wrap_add(t, tb.shift[e], tb.z);
+    }
     static constexpr bool fixed = true;
+};
+
+// A code compiled in completely (C = Code11ad12, ...): every column and
+// shift is an immediate.
+template <class C>
+struct CompiledShape {
+    static constexpr int L = C::L;
+    static constexpr int E = C::E;
+    static constexpr int E_REG = C::E;
+    static constexpr int D = C::D;
+    __host__ __device__ static constexpr int maxd(int l) { return C::maxd(l); }
+    __host__ __device__ static constexpr int slot(int l, int j) { return C::slot(l, j); }
+    __device__ static bool has(const OmsTables&, int, int) { return true; }
+    __device__ static int addr(const OmsTables&, int e, int t, int gbase) {
+        return gbase + C::col(e) * C::Z + wrap_add(t, C::shift(e), C::Z);
+    }
+    static constexpr bool fixed = true;
+};
+
+// Compiled code with the check messages of edge slots >= EREG kept in shared
+// memory instead of registers (fewer registers, more resident warps).
+template <class C, int EREG>
+struct SplitShape : CompiledShape<C> {
+    static constexpr int E_REG = EREG;
 };
 
 template <int L_, int D_>
@@ -87,6 +137,7 @@ struct PaddedShape {
     static constexpr int L = L_;
     static constexpr int D = D_;
     static constexpr int E = L_ * D_;
+    static constexpr int E_REG = E;
     __host__ __device__ static constexpr int maxd(int) { return D_; }
     __host__ __device__ static constexpr int slot(int l, int j) { return l * D_ + j; }
     __device__ static bool has(const OmsTables& tb, int l, int j) {
@@ -94,62 +145,72 @@ struct PaddedShape {
         asm volatile("" : "+r"(d));   // re-read per layer pass instead of keeping L*D predicates live
         return j < d;
     }
+    __device__ static int addr(const OmsTables& tb, int e, int t, int gbase) {
+        return gbase + tb.colz[e] + wrap_add(t, tb.shift[e], tb.z);
+    }
     static constexpr bool fixed = false;
 };
 
 struct OmsConsts {
-    __half2 lo, hi, zero2, beta2, maxv2;
+    uint32_t beta2, maxv2;
+    uint32_t* Rs;        // shared-memory messages of edge slots >= E_REG: Rs[(e - E_REG) * nthreads]
 };
+
+template <class S>
+__device__ __forceinline__ uint32_t get_r(const uint32_t (&R)[S::E_REG > 0 ? S::E_REG : 1], const OmsConsts& k, int e) {
+    if (e < S::E_REG) return R[e < S::E_REG ? e : 0];
+    return k.Rs[(e - S::E_REG) * blockDim.x];
+}
+template <class S>
+__device__ __forceinline__ void set_r(uint32_t (&R)[S::E_REG > 0 ? S::E_REG : 1], const OmsConsts& k, int e, uint32_t v) {
+    if (e < S::E_REG) R[e < S::E_REG ? e : 0] = v;
+    else k.Rs[(e - S::E_REG) * blockDim.x] = v;
+}
 
 // One layer of the layered update for this thread's check row t (all edges
 // of the row; the layer index is a template argument so every message
 // register index is a compile-time constant).
 template <class S, bool BETA0, int l>
-__device__ __forceinline__ void oms_layer(const OmsTables& tb, uint32_t* Ps, uint32_t (&R)[S::E], int t, int gbase,
+__device__ __forceinline__ void oms_layer(const OmsTables& tb, uint32_t* Ps, uint32_t (&R)[S::E_REG > 0 ? S::E_REG : 1], int t, int gbase,
                                           const OmsConsts& k) {
     constexpr int D = S::maxd(l);
     constexpr uint32_t SGN = 0x80008000u;
-    const int z = tb.z;
     uint32_t q[D];
     int addr[D];
-    __half2 mn1 = __float2half2_rn(1024.0f), mn2 = mn1;
+    uint32_t mn1 = H2_1024, mn2 = H2_1024;
     uint32_t sx = 0;
 #pragma unroll
     for (int j = 0; j < D; ++j) {
         if (S::has(tb, l, j)) {
             const int e = S::slot(l, j);
-            int v = t + tb.shift[e];
-            v = v >= z ? v - z : v;
-            addr[j] = gbase + tb.colz[e] + v;
-            __half2 Q = __hsub2(u2h(Ps[addr[j]]), u2h(R[e]));
-            Q = __hmin2(__hmax2(Q, k.lo), k.hi);
-            const __half2 a = abs_q<BETA0>(Q);
-            mn2 = __hmin2(mn2, __hmax2(mn1, a));
-            mn1 = __hmin2(mn1, a);
-            q[j] = h2u(Q);
-            sx ^= q[j];
+            addr[j] = S::addr(tb, e, t, gbase);
+            uint32_t Q = hsub2(Ps[addr[j]], get_r<S>(R, k, e));
+            Q = hmin2(hmax2(Q, H2_M128), H2_P127);
+            const uint32_t a = abs_q<BETA0>(Q);
+            mn2 = hmin2(mn2, hmax2(mn1, a));
+            mn1 = hmin2(mn1, a);
+            q[j] = Q;
+            sx ^= Q;
         }
     }
-    const __half2 c1 = __hmin2(__hmax2(__hsub2(mn1, k.beta2), k.zero2), k.maxv2);
-    const __half2 c2 = __hmin2(__hmax2(__hsub2(mn2, k.beta2), k.zero2), k.maxv2);
-    const uint32_t X = h2u(c1) ^ h2u(c2);
-    const uint32_t M1 = h2u(c1) ^ (sx & SGN);
+    const uint32_t c1 = hmin2(hmax2(hsub2(mn1, k.beta2), H2_ZERO), k.maxv2);
+    const uint32_t c2 = hmin2(hmax2(hsub2(mn2, k.beta2), H2_ZERO), k.maxv2);
+    const uint32_t X = c1 ^ c2;
+    const uint32_t M1 = c1 ^ (sx & SGN);
 #pragma unroll
     for (int j = 0; j < D; ++j) {
         if (S::has(tb, l, j)) {
-            const __half2 Q = u2h(q[j]);
-            const uint32_t eq = __heq2_mask(abs_q<BETA0>(Q), mn1);
+            const uint32_t eq = heq2_mask(abs_q<BETA0>(q[j]), mn1);
             const uint32_t Rn = M1 ^ (q[j] & SGN) ^ (eq & X);
-            __half2 Pn = __hadd2(Q, u2h(Rn));
-            Pn = __hmin2(__hmax2(Pn, k.lo), k.hi);
-            Ps[addr[j]] = h2u(Pn);
-            R[S::slot(l, j)] = Rn;
+            const uint32_t Pn = hmin2(hmax2(hadd2(q[j], Rn), H2_M128), H2_P127);
+            Ps[addr[j]] = Pn;
+            set_r<S>(R, k, S::slot(l, j), Rn);
         }
     }
 }
 
 template <class S, bool BETA0, int l>
-__device__ __forceinline__ void oms_layer_sync(const OmsTables& tb, uint32_t* Ps, uint32_t (&R)[S::E], int t, int gbase,
+__device__ __forceinline__ void oms_layer_sync(const OmsTables& tb, uint32_t* Ps, uint32_t (&R)[S::E_REG > 0 ? S::E_REG : 1], int t, int gbase,
                                                bool active, const OmsConsts& k) {
     if (active) oms_layer<S, BETA0, l>(tb, Ps, R, t, gbase, k);
     __syncthreads();
@@ -157,7 +218,7 @@ __device__ __forceinline__ void oms_layer_sync(const OmsTables& tb, uint32_t* Ps
 
 template <class S, bool BETA0, int... ls>
 __device__ __forceinline__ void oms_iteration(std::integer_sequence<int, ls...>, const OmsTables& tb, uint32_t* Ps,
-                                              uint32_t (&R)[S::E], int t, int gbase, bool active, const OmsConsts& k) {
+                                              uint32_t (&R)[S::E_REG > 0 ? S::E_REG : 1], int t, int gbase, bool active, const OmsConsts& k) {
     (oms_layer_sync<S, BETA0, ls>(tb, Ps, R, t, gbase, active, k), ...);
 }
 
@@ -168,87 +229,131 @@ __device__ __forceinline__ uint32_t oms_row_parity(const OmsTables& tb, const ui
     uint32_t x = 0;
 #pragma unroll
     for (int j = 0; j < S::maxd(l); ++j) {
-        if (S::has(tb, l, j)) {
-            const int e = S::slot(l, j);
-            int v = t + tb.shift[e];
-            v = v >= tb.z ? v - tb.z : v;
-            x ^= Ps[gbase + tb.colz[e] + v];
-        }
+        if (S::has(tb, l, j)) x ^= Ps[S::addr(tb, S::slot(l, j), t, gbase)];
     }
     return x;
 }
 
-template <class S, int... ls>
-__device__ __forceinline__ uint32_t oms_syndrome(std::integer_sequence<int, ls...>, const OmsTables& tb, const uint32_t* Ps,
-                                                 int t, int gbase) {
-    return (oms_row_parity<S, ls>(tb, Ps, t, gbase) | ...);
+// Syndrome with early exit: a thread publishes failing parity checks as soon
+// as it finds them and stops once both lanes of its group are known to fail
+// (the result, "some check of this codeword fails", is the same).
+template <class S, int l>
+__device__ __forceinline__ void oms_syndrome_step(const OmsTables& tb, const uint32_t* Ps, int t, int gbase,
+                                                  uint32_t* synd, uint32_t& seen, bool& stop) {
+    if (stop) return;
+    const uint32_t x = oms_row_parity<S, l>(tb, Ps, t, gbase) & 0x80008000u;
+    if (x & ~seen) {
+        atomicOr(synd, x);
+        seen |= x;
+    }
+    if (((seen | *reinterpret_cast<volatile uint32_t*>(synd)) & 0x80008000u) == 0x80008000u) stop = true;
 }
 
-template <class S, bool BETA0, int MAXT>
-__global__ void __launch_bounds__(MAXT, 1) oms_f16_kernel(const __grid_constant__ OmsTables tb, const __grid_constant__ OmsJob job) {
+template <class S, int... ls>
+__device__ __forceinline__ void oms_syndrome(std::integer_sequence<int, ls...>, const OmsTables& tb, const uint32_t* Ps,
+                                             int t, int gbase, uint32_t* synd) {
+    uint32_t seen = 0;
+    bool stop = false;
+    (oms_syndrome_step<S, ls>(tb, Ps, t, gbase, synd, seen, stop), ...);
+}
+
+// ---- asynchronous global -> shared copies (prefetch of the next codeword) ----
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Copy codeword cw's n LLR bytes into a staging buffer (16-byte chunks when n
+// is a multiple of 16, else 4-byte chunks, else single bytes).
+// The staging buffer is 16-byte aligned; the source must be too for the
+// wide path (n and the llr base pointer are checked).
+__device__ __forceinline__ void prefetch_llr(int8_t* stage, const int8_t* llr, long long cw, int n, int lane) {
+    const int8_t* src = llr + cw * (long long)n;
+    const unsigned long long base = reinterpret_cast<unsigned long long>(llr);
+    if ((n & 15) == 0 && (base & 15) == 0) {
+        for (int i = 16 * lane; i < n; i += 512) cp_async16(stage + i, src + i);
+    } else if ((n & 3) == 0 && (base & 3) == 0) {
+        for (int i = 4 * lane; i < n; i += 128) cp_async4(stage + i, src + i);
+    } else {
+        for (int i = lane; i < n; i += 32) stage[i] = src[i];
+    }
+}
+
+template <class S, bool BETA0, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) oms_f16_kernel(const __grid_constant__ OmsTables tb, const __grid_constant__ OmsJob job) {
+    // dynamic shared memory: posteriors [G][stride] words, then LLR staging [2G][nstage] bytes
     extern __shared__ uint32_t Ps[];
-    __shared__ long long s_cw[32];       // codeword decoded by slot (-1 = empty)
-    __shared__ long long s_fin_cw[32];   // codeword finished at this boundary (-1 = none)
+    __shared__ long long s_cur[32];      // codeword decoded by slot (-1 = none)
+    __shared__ long long s_next[32];     // codeword prefetched for the slot (-1 = none)
     __shared__ int s_it[32];
-    __shared__ int s_fin_it[32];
-    __shared__ int s_new[32];            // slot received a new codeword at this boundary
-    __shared__ uint32_t s_synd[16];
-    __shared__ uint32_t s_zero_mask[16]; // per group: half-lanes whose R must be cleared
-    __shared__ int s_continue;
+    // per iteration parity p: failing-check bits and R-clear masks per group, busy flag
+    __shared__ uint32_t s_synd[2][16];
+    __shared__ uint32_t s_zero_mask[2][16];
+    __shared__ int s_busy[2];
+    __shared__ unsigned long long s_head;   // next unclaimed codeword of this CTA's range
     __shared__ unsigned long long s_cnt[OMS_MAX_BUCKETS][4];
 
     const int z = tb.z, n = tb.n, G = tb.G, stride = tb.stride;
     const int nslots = 2 * G;
+    const int nstage = (n + 15) & ~15;
+    int8_t* stage_base = reinterpret_cast<int8_t*>(Ps) + ((G * stride * 4 + 15) & ~15);
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const int nwarps = blockDim.x >> 5;
     const int t = tid / G, g = tid - (tid / G) * G;
     const bool active = t < z;
     const int gbase = g * stride;
+    // this CTA's contiguous share of the codewords (static: no global atomics)
+    const long long lo = job.ncw * blockIdx.x / gridDim.x, hi = job.ncw * (blockIdx.x + 1) / gridDim.x;
 
     for (int i = tid; i < OMS_MAX_BUCKETS * 4; i += blockDim.x) (&s_cnt[0][0])[i] = 0;
     for (int i = tid; i < G * stride; i += blockDim.x) Ps[i] = 0;
-    if (tid < 16) { s_synd[tid] = 0; s_zero_mask[tid] = 0; }
-    __syncthreads();
-
-    // ---- initial claim: warp 0 takes one codeword per slot
-    if (warp == 0) {
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(job.queue, (unsigned long long)nslots);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (lane < nslots) {
-            long long cw = (long long)base + lane;
-            s_cw[lane] = cw < job.ncw ? cw : -1;
-            s_it[lane] = 0;
-            s_new[lane] = cw < job.ncw;
+    if (tid < 32) {
+        const long long c0 = lo + tid, c1 = lo + nslots + tid;
+        const bool ok = tid < nslots;
+        s_cur[tid] = ok && c0 < hi ? c0 : -1;
+        s_next[tid] = ok && c1 < hi ? c1 : -1;
+        s_it[tid] = 0;
+        if (tid < 16) {
+            s_synd[0][tid] = s_synd[1][tid] = 0;
+            s_zero_mask[0][tid] = s_zero_mask[1][tid] = 0;
         }
+        if (tid < 2) s_busy[tid] = 0;
     }
+    if (tid == 0) s_head = (unsigned long long)(lo + 2 * nslots);
     __syncthreads();
 
-    // ---- load helper: slot k's LLRs into its half-lane of group k>>1
-    auto refill = [&](int k) {
-        const long long cw = s_cw[k];
-        const int gg = k >> 1;
-        __half* dst = reinterpret_cast<__half*>(Ps + gg * stride) + (k & 1);
-        const int8_t* src = job.llr + cw * (long long)n;
-        for (int i = lane; i < n; i += 32) dst[2 * i] = __int2half_rn((int)src[i]);
-    };
-    for (int k = warp; k < nslots; k += nwarps)
-        if (s_new[k]) refill(k);
+    // initial codewords straight into the posteriors; prefetch the second round
+    for (int k = warp; k < nslots; k += nwarps) {
+        const long long cw = s_cur[k];
+        if (cw >= 0) {
+            __half* dst = reinterpret_cast<__half*>(Ps + (k >> 1) * stride) + (k & 1);
+            const int8_t* src = job.llr + cw * (long long)n;
+            for (int i = lane; i < n; i += 32) dst[2 * i] = __int2half_rn((int)src[i]);
+        }
+        if (s_next[k] >= 0) prefetch_llr(stage_base + k * nstage, job.llr, s_next[k], n, lane);
+    }
+    cp_async_commit();
     __syncthreads();
 
-    uint32_t R[S::E];
+    uint32_t R[S::E_REG > 0 ? S::E_REG : 1];
 #pragma unroll
-    for (int e = 0; e < S::E; ++e) R[e] = 0u;
+    for (int e = 0; e < (S::E_REG > 0 ? S::E_REG : 1); ++e) R[e] = 0u;
 
     OmsConsts kc;
-    kc.lo = __float2half2_rn(-128.0f);
-    kc.hi = __float2half2_rn(127.0f);
-    kc.zero2 = __float2half2_rn(0.0f);
-    kc.beta2 = u2h(job.beta2);
-    kc.maxv2 = u2h(job.maxv2);
+    kc.beta2 = job.beta2;
+    kc.maxv2 = job.maxv2;
+    // shared-memory messages after the LLR staging area
+    kc.Rs = reinterpret_cast<uint32_t*>(stage_base + 2 * G * nstage) + tid;
+    for (int e = S::E_REG; e < S::E; ++e) kc.Rs[(e - S::E_REG) * blockDim.x] = 0u;
 
-    while (true) {
+    for (int par = 0;; par ^= 1) {
         // ================= one layered iteration =================
         // Per-edge addresses are recomputed every iteration rather than kept
         // live across it (they would need a register per edge): hide t and
@@ -256,112 +361,107 @@ __global__ void __launch_bounds__(MAXT, 1) oms_f16_kernel(const __grid_constant_
         int t_it = t, gbase_it = gbase;
         asm volatile("" : "+r"(t_it), "+r"(gbase_it));
         oms_iteration<S, BETA0>(std::make_integer_sequence<int, S::L>(), tb, Ps, R, t_it, gbase_it, active, kc);
+        // (the layer loop ends with a barrier) buffers of the other parity are free again
+        if (tid < 16) {
+            s_synd[par ^ 1][tid] = 0;
+            s_zero_mask[par ^ 1][tid] = 0;
+        }
+        if (tid == 0) s_busy[par ^ 1] = 0;
 
         // ================= syndrome of every slot =================
-        if (active) {
-            const uint32_t acc = oms_syndrome<S>(std::make_integer_sequence<int, S::L>(), tb, Ps, t_it, gbase_it) & 0x80008000u;
-            if (acc) atomicOr(&s_synd[g], acc);
-        }
+        if (active) oms_syndrome<S>(std::make_integer_sequence<int, S::L>(), tb, Ps, t_it, gbase_it, &s_synd[par][g]);
         __syncthreads();
 
-        // ================= slot bookkeeping (warp 0) =================
-        if (warp == 0) {
-            const int k = lane;
-            const bool valid = k < nslots;
-            long long cw = valid ? s_cw[k] : -1;
-            bool done = false;
-            int it = 0;
-            if (cw >= 0) {
-                it = s_it[k] + 1;
-                const uint32_t bit = (k & 1) ? 0x80000000u : 0x00008000u;
-                done = !(s_synd[k >> 1] & bit) || it >= job.max_iter;
-            }
-            const unsigned dm = __ballot_sync(0xffffffffu, done);
-            unsigned long long base = 0;
-            if (dm) {
-                if (lane == 0) base = atomicAdd(job.queue, (unsigned long long)__popc(dm));
-                base = __shfl_sync(0xffffffffu, base, 0);
-            }
-            long long ncw_new = -1;
-            if (done) {
-                const long long c = (long long)base + __popc(dm & ((1u << lane) - 1u));
-                ncw_new = c < job.ncw ? c : -1;
-            }
-            if (valid) {
-                s_fin_cw[k] = done ? cw : -1;
-                s_fin_it[k] = it;
-                s_cw[k] = done ? ncw_new : cw;
-                s_it[k] = done ? 0 : it;
-                s_new[k] = done && ncw_new >= 0;
-            }
-            const unsigned busy = __ballot_sync(0xffffffffu, valid && (done ? ncw_new >= 0 : cw >= 0));
-            // per group: clear R in half-lanes that finished
-            const unsigned dpair = dm >> (2 * (lane & 15));
-            if (lane < G) {
-                s_zero_mask[lane] = ((dpair & 1u) ? 0x0000ffffu : 0u) | ((dpair & 2u) ? 0xffff0000u : 0u);
-                s_synd[lane] = 0;
-            }
-            if (lane == 0) s_continue = busy != 0;
-        }
-        __syncthreads();
-
-        // ================= write finished codewords, refill slots =================
+        // ====== each warp: its slots -- decide, write out, promote, claim, prefetch ======
+        cp_async_wait_all();   // this warp's prefetches (issued an iteration ago)
+        __syncwarp();
         for (int k = warp; k < nslots; k += nwarps) {
-            const long long cw = s_fin_cw[k];
-            if (cw >= 0) {
-                const int gg = k >> 1, hsel = k & 1;
-                const __half* src = reinterpret_cast<const __half*>(Ps + gg * stride) + hsel;
-                // hard decisions of the data columns, 32 per ballot
-                uint32_t mine = 0, errw = 0;
-                unsigned errslots = 0;
-                const uint32_t* ref = job.ref_bits ? job.ref_bits + (cw % job.ref_period) * tb.hard_words : nullptr;
-                for (int w = 0; w < tb.hard_words; ++w) {
-                    const int i = w * 32 + lane;
-                    bool b = false;
-                    if (i < tb.kbits) b = __hlt(src[2 * i], __float2half(0.0f));
+            const long long cw = s_cur[k];
+            if (cw < 0) continue;
+            const int gg = k >> 1, hsel = k & 1;
+            const int it = s_it[k] + 1;
+            const uint32_t bit = hsel ? 0x80000000u : 0x00008000u;
+            const bool done = !(s_synd[par][gg] & bit) || it >= job.max_iter;
+            if (!done) {
+                if (lane == 0) { s_it[k] = it; s_busy[par] = 1; }
+                continue;
+            }
+            __half* pk = reinterpret_cast<__half*>(Ps + gg * stride) + hsel;
+            // hard decisions of the data columns, 32 per ballot
+            const uint32_t* ref = job.ref_bits ? job.ref_bits + (cw % job.ref_period) * tb.hard_words : nullptr;
+            uint32_t mine = 0, refw = 0, errw = 0;
+            unsigned errslots = 0;
+            for (int w0 = 0; w0 < tb.hard_words; w0 += 32) {
+                if (ref && w0 + lane < tb.hard_words) refw = ref[w0 + lane];
+                const int wn = min(32, tb.hard_words - w0);
+                for (int w = 0; w < wn; ++w) {
+                    const int i = (w0 + w) * 32 + lane;
+                    const bool b = (i < tb.kbits) && __hlt(pk[2 * i], __float2half(0.0f));
                     const uint32_t word = __ballot_sync(0xffffffffu, b);
-                    if (lane == (w & 31)) mine = word;
-                    if (job.hard_out && ((w & 31) == 31 || w == tb.hard_words - 1) && lane <= (w & 31))
-                        job.hard_out[cw * tb.hard_words + (w & ~31) + lane] = mine;
+                    if (lane == w) mine = word;
                     if (ref) {
-                        const uint32_t rw = ref[w];
+                        const uint32_t rw = __shfl_sync(0xffffffffu, refw, w);
                         const bool e = (i < tb.kbits) && (b != (bool)((rw >> lane) & 1u));
                         if (e) errslots |= 1u << ((i % z) % job.num_par);
                         errw += __popc(__ballot_sync(0xffffffffu, e));
                     }
                 }
-                if (job.post_out) {
-                    int8_t* dst = job.post_out + cw * (long long)n;
-                    for (int i = lane; i < n; i += 32) dst[i] = (int8_t)__half2int_rn(src[2 * i]);
-                }
-                if (lane == 0 && job.iters_out) job.iters_out[cw] = (uint8_t)s_fin_it[k];
-                if (job.counters) {
-                    const unsigned slots = __reduce_or_sync(0xffffffffu, errslots);
-                    if (lane == 0) {
-                        int b = (int)(cw / job.bucket_size);
-                        b = b < job.n_buckets ? b : job.n_buckets - 1;
-                        atomicAdd(&s_cnt[b][0], 1ull);
-                        atomicAdd(&s_cnt[b][1], (unsigned long long)s_fin_it[k]);
-                        if (errw) {
-                            atomicAdd(&s_cnt[b][2], (unsigned long long)errw);
-                            atomicAdd(&s_cnt[b][3], (unsigned long long)__popc(slots));
-                        }
+                if (job.hard_out && lane < wn) job.hard_out[cw * tb.hard_words + w0 + lane] = mine;
+            }
+            if (job.post_out) {
+                int8_t* dst = job.post_out + cw * (long long)n;
+                for (int i = lane; i < n; i += 32) dst[i] = (int8_t)__half2int_rn(pk[2 * i]);
+            }
+            if (lane == 0 && job.iters_out) job.iters_out[cw] = (uint8_t)it;
+            if (job.counters) {
+                const unsigned slots = __reduce_or_sync(0xffffffffu, errslots);
+                if (lane == 0) {
+                    int bk = (int)(cw / job.bucket_size);
+                    bk = bk < job.n_buckets ? bk : job.n_buckets - 1;
+                    atomicAdd(&s_cnt[bk][0], 1ull);
+                    atomicAdd(&s_cnt[bk][1], (unsigned long long)it);
+                    if (errw) {
+                        atomicAdd(&s_cnt[bk][2], (unsigned long long)errw);
+                        atomicAdd(&s_cnt[bk][3], (unsigned long long)__popc(slots));
                     }
                 }
             }
             __syncwarp();
-            if (s_new[k]) refill(k);
-        }
-        __syncthreads();
-        if (active) {
-            const uint32_t m = s_zero_mask[g];
-            if (m) {
-#pragma unroll
-                for (int e = 0; e < S::E; ++e) R[e] &= ~m;
+            // promote the prefetched codeword, claim and prefetch the one after it
+            const long long nxt = s_next[k];
+            if (nxt >= 0) {
+                const int8_t* st = stage_base + k * nstage;
+                for (int i = lane; i < n; i += 32) pk[2 * i] = __int2half_rn((int)st[i]);
+                __syncwarp();
+                unsigned long long c = 0;
+                if (lane == 0) c = atomicAdd(&s_head, 1ull);
+                c = __shfl_sync(0xffffffffu, c, 0);
+                const long long fresh = (long long)c < hi ? (long long)c : -1;
+                if (fresh >= 0) prefetch_llr(stage_base + k * nstage, job.llr, fresh, n, lane);
+                if (lane == 0) {
+                    s_next[k] = fresh;
+                    s_busy[par] = 1;
+                }
+            }
+            if (lane == 0) {
+                s_cur[k] = nxt;
+                s_it[k] = 0;
+                atomicOr(&s_zero_mask[par][gg], hsel ? 0xffff0000u : 0x0000ffffu);
             }
         }
-        if (!s_continue) break;
+        cp_async_commit();
+        __syncthreads();
+        if (active) {
+            const uint32_t m = s_zero_mask[par][g];
+            if (m) {
+#pragma unroll
+                for (int e = 0; e < S::E_REG; ++e) R[e] &= ~m;
+                for (int e = S::E_REG; e < S::E; ++e) kc.Rs[(e - S::E_REG) * blockDim.x] &= ~m;
+            }
+        }
+        if (!s_busy[par]) break;
     }
+    cp_async_wait_all();
 
     if (job.counters) {
         __syncthreads();

@@ -110,3 +110,44 @@ def test_compat_reference_layout(capi, oracle):
     post_o, it_o = oracle.decode_int8(code, llr, 10, 31.0, 1.0)
     assert tot == int(it_o.sum())
     assert np.array_equal(buf[:, :, P:P + code.z].reshape(n, code.n), post_o)
+
+
+def test_unaligned_llr_pointer(capi, oracle):
+    """Device LLRs starting at an odd address take the byte-copy prefetch path."""
+    import torch
+    from ldpc_b200 import codes
+    code = codes.make_code("11ad 1/2")
+    llr, _, _ = make_llr_int8(code, 200, -0.5, seed=13, oracle=oracle)
+    ctx = _ctx(capi, code)
+    buf = torch.zeros(llr.size + 1, dtype=torch.int8, device="cuda")
+    buf[1:] = torch.from_numpy(llr.ravel()).cuda()
+    iters = torch.empty(llr.shape[0], dtype=torch.uint8, device="cuda")
+    post = torch.empty(llr.shape, dtype=torch.int8, device="cuda")
+    ctx.decode_int8(buf.data_ptr() + 1, llr.shape[0], post, None, iters)
+    torch.cuda.synchronize()
+    post_o, it_o = oracle.decode_int8(code, llr, 10, 31.0, 1.0)
+    assert np.array_equal(post.cpu().numpy(), post_o)
+    assert np.array_equal(iters.cpu().numpy(), it_o.astype(np.uint8))
+
+
+def test_fused_error_counting(capi, oracle):
+    """ldpc_decode_count: per-bucket codewords/iterations/bit and codeword errors."""
+    import torch
+    from ldpc_b200 import codes
+    code = codes.make_code("11ad 1/2")
+    n = 1500
+    llr, info, _ = make_llr_int8(code, n, -1.0, seed=17, oracle=oracle)
+    ctx = _ctx(capi, code)
+    data = torch.from_numpy(pack_bits(info).view(np.int32)).cuda()
+    cnt = torch.zeros((3, 4), dtype=torch.int64, device="cuda")
+    ctx.decode_count(torch.from_numpy(llr).cuda(), n, data_bits=data, ref_period=n, bucket_size=500, counters=cnt,
+                     n_buckets=3)
+    torch.cuda.synchronize()
+    post_o, it_o = oracle.decode_int8(code, llr, 10, 31.0, 1.0)
+    c = cnt.cpu().numpy()
+    for b in range(3):
+        sl = slice(500 * b, 500 * (b + 1))
+        cw_err, bit_err = oracle.count_errors(code, post_o[sl], np.concatenate(
+            [info[sl], np.zeros((500, code.n - info.shape[1]), np.uint8)], axis=1))
+        assert c[b, 0] == 500 and c[b, 1] == int(it_o[sl].sum())
+        assert c[b, 2] == bit_err and c[b, 3] == cw_err
