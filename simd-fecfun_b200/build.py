@@ -49,6 +49,9 @@ def _compile(src: str, force: bool, hdr_time: float, verbose: bool) -> str:
 
 def build(force: bool = False, jobs: int = 8, verbose: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
+    sys.path.insert(0, HERE)
+    import gen_trees
+    gen_trees.generate(os.path.join(CSRC, "gen_trees.cuh"))
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     hdr = _newest_header()
     with ThreadPoolExecutor(max_workers=jobs) as ex:

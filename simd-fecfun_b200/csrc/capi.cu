@@ -302,8 +302,10 @@ int ldpc_ctx_create(const ldpc_code* code, const ldpc_cfg* cfg, int device, ldpc
     CUDA_TRY(cudaEventCreate(&x->ev_start));
     CUDA_TRY(cudaEventCreate(&x->ev_stop));
     if (code->has_enc) {
-        int rc = ldpc::setup_gen(x.get());
-        if (rc) return rc;
+        // the generator is optional: a code whose schedule it cannot hold still decodes
+        x->gen_ok = ldpc::setup_gen(x.get()) == LDPC_OK;
+        if (!x->gen_ok) x->gen_err = g_err;
+        g_err.clear();
     }
     *out = x.release();
     return LDPC_OK;
@@ -315,6 +317,7 @@ void ldpc_ctx_destroy(ldpc_ctx* x) {
     cudaFree(x->d_queue);
     cudaFree(x->d_status);
     cudaFree(x->d_counters);
+    cudaFree(x->d_sp_scratch);
     for (int i = 0; i < 2; ++i) {
         if (x->streams[i]) cudaStreamDestroy(x->streams[i]);
         for (int k = 0; k < 4; ++k) cudaFree(x->d_pipe[i][k]);

@@ -81,6 +81,7 @@ void release_gen(ldpc_ctx* x) {
 int launch_gen(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* snr_db, size_t n_snr, size_t n_per_snr,
                int8_t* llr_i8, float* llr_f32, uint32_t* data_bits, unsigned long long* uncoded, cudaStream_t s) {
     if (!x->code.has_enc) return fail(LDPC_ERR_INVALID_ARG, "code has no encoder table");
+    if (!x->gen_ok) return fail(LDPC_ERR_UNSUPPORTED, "generator: %s", x->gen_err.c_str());
     if (n_snr < 1 || n_snr > (size_t)GEN_MAX_SNR) return fail(LDPC_ERR_INVALID_ARG, "n_snr=%zu outside 1..%d", n_snr, GEN_MAX_SNR);
     if (!snr_db) return fail(LDPC_ERR_INVALID_ARG, "snr_db is NULL");
     if (n_per_snr == 0) return LDPC_OK;
@@ -120,6 +121,7 @@ int ldpc_generate(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* s
 int ldpc_encode(ldpc_ctx* x, const uint32_t* data_bits, size_t n, uint8_t* cw_bits, void* stream) {
     if (!x) return fail(LDPC_ERR_INVALID_ARG, "ctx is NULL");
     if (!x->code.has_enc) return fail(LDPC_ERR_INVALID_ARG, "code has no encoder table");
+    if (!x->gen_ok) return fail(LDPC_ERR_UNSUPPORTED, "encoder: %s", x->gen_err.c_str());
     if (n == 0) return LDPC_OK;
     if (!data_bits || !cw_bits) return fail(LDPC_ERR_INVALID_ARG, "NULL buffer");
     CUDA_TRY(cudaSetDevice(x->device));
@@ -134,6 +136,7 @@ int ldpc_llr_from_noise(ldpc_ctx* x, const uint8_t* cw_bits, const float* noise,
                         float* llr_f32, unsigned long long* uncoded, void* stream) {
     if (!x) return fail(LDPC_ERR_INVALID_ARG, "ctx is NULL");
     if (!x->code.has_enc) return fail(LDPC_ERR_INVALID_ARG, "code has no encoder table (puncture/filler masks)");
+    if (!x->gen_ok) return fail(LDPC_ERR_UNSUPPORTED, "generator: %s", x->gen_err.c_str());
     if (n == 0) return LDPC_OK;
     if (!cw_bits || !noise || (!llr_i8 && !llr_f32)) return fail(LDPC_ERR_INVALID_ARG, "NULL buffer");
     CUDA_TRY(cudaSetDevice(x->device));

@@ -88,9 +88,12 @@ struct ldpc_ctx {
     ldpc::SpTables spt;
     ldpc::sp_fn sp_kernel = nullptr;
     int sp_threads = 0, sp_smem = 0, sp_ctas = 0;
+    float* d_sp_scratch = nullptr;              // check messages of large codes (global)
     float maxf = 0.f;
     // generation
     ldpc::GenTables gent;
+    bool gen_ok = false;                        // generator/encoder usable for this code
+    std::string gen_err;
     uint8_t* d_masks = nullptr;                 // punct[n] then filler[n]
     void* d_sim_llr = nullptr;                  // ldpc_simulate scratch: LLRs of one chunk, all SNR points
     void* d_sim_data = nullptr;                 //   sent data bits of the chunk

@@ -1,0 +1,242 @@
+// Layered float32 decoders: sum-product (tanh / product tree / 2 atanh) and
+// offset min-sum, bit-exact with the reference's SIMD_ELEM_BW=-32 builds
+// (LDPCtop_Vec16f_prod, LDPCtop_Vec16f_min):
+//   Q = P - R                                  decode_functions.cpp:53
+//   a = max(|Q| - beta, 0)                     :56-62
+//   x = tanh(a/2) (sum-product) or a           min_find.pl:37-41
+//   f_j = combine over k != j, fixed tree      min_find.pl:52-164 (gen_trees.cuh)
+//         clamped at Max_val, then 2 atanh(.)  min_find.pl:99-107, 44-45
+//   R' = f_j with the sign of prod_{k!=j} Q_k  decode_functions.cpp:85-87
+//   P  = Q + R'                                :91
+// with the same float operations in the same order as the oracle (no fused
+// multiply-adds; tanh/atanh from ldpc_math.h), so posteriors agree bit for bit.
+//
+// Work layout: G codewords per CTA, one per group of Z threads (thread
+// (t, g) = check row t of every layer).  Posteriors in shared memory, check
+// messages in shared memory (RSMEM) or, for large codes, in a global scratch
+// area; the layer loop runs over run-time tables, so any code shape works.
+// The iteration boundary (syndrome, write-out, refill from a prefetched
+// staging buffer) follows the int8 kernel.
+#pragma once
+#include <stdint.h>
+
+#include "gen_trees.cuh"
+#include "ldpc_math.h"
+#include "tables.h"
+
+namespace ldpc {
+
+__device__ __forceinline__ int sp_wrap(int t, int s, int z) { return (int)min((unsigned)(t + s), (unsigned)(t + s - z)); }
+
+__device__ __forceinline__ void sp_cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void sp_cp_async4(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void sp_prefetch(float* stage, const float* llr, long long cw, int n, int lane) {
+    const float* src = llr + cw * (long long)n;
+    const unsigned long long base = reinterpret_cast<unsigned long long>(src);
+    if ((n & 3) == 0 && (base & 15) == 0) {
+        for (int i = 4 * lane; i < n; i += 128) sp_cp_async16(stage + i, src + i);
+    } else {
+        for (int i = lane; i < n; i += 32) sp_cp_async4(stage + i, src + i);
+    }
+}
+
+template <int DMAX, bool PROD, bool RSMEM, int MAXT>
+__global__ void __launch_bounds__(MAXT) sp_f32_kernel(const __grid_constant__ SpTables tb, const __grid_constant__ SpJob job) {
+    extern __shared__ float sm_f[];
+    __shared__ long long s_cur[32];
+    __shared__ long long s_next[32];
+    __shared__ int s_it[32];
+    __shared__ uint32_t s_synd[2];        // bit g: a check of group g's codeword fails (per iteration parity)
+    __shared__ uint32_t s_zero[2];        // bit g: clear group g's messages
+    __shared__ int s_busy[2];
+    __shared__ unsigned long long s_head;
+    __shared__ unsigned long long s_cnt[OMS_MAX_BUCKETS][4];
+
+    const int z = tb.z, n = tb.n, G = tb.G, stride = tb.stride;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
+    const int nthr = blockDim.x;
+    const int t = tid / G, g = tid - (tid / G) * G;
+    const bool active = t < z;
+    const int gbase = g * stride;
+    float* Ps = sm_f;
+    float* stage = sm_f + ((G * stride + 3) & ~3);                  // [G][nstage], 16-byte aligned
+    const int nstage = (n + 3) & ~3;
+    float* Rbase = RSMEM ? stage + G * nstage : job.r_scratch + (long long)blockIdx.x * tb.E * nthr;
+    float* Rt = Rbase + tid;                                        // message of edge e at Rt[e * nthr]
+    const long long lo = job.ncw * blockIdx.x / gridDim.x, hi = job.ncw * (blockIdx.x + 1) / gridDim.x;
+    const float beta = job.beta, maxv = job.maxv;
+
+    for (int i = tid; i < OMS_MAX_BUCKETS * 4; i += nthr) (&s_cnt[0][0])[i] = 0;
+    for (int i = tid; i < G * stride; i += nthr) Ps[i] = 0.f;
+    for (int e = 0; e < tb.E; ++e) Rt[e * nthr] = 0.f;
+    if (tid < 32) {
+        const long long c0 = lo + tid, c1 = lo + G + tid;
+        s_cur[tid] = tid < G && c0 < hi ? c0 : -1;
+        s_next[tid] = tid < G && c1 < hi ? c1 : -1;
+        s_it[tid] = 0;
+    }
+    if (tid < 2) { s_synd[tid] = 0; s_zero[tid] = 0; s_busy[tid] = 0; }
+    if (tid == 0) s_head = (unsigned long long)(lo + 2 * G);
+    __syncthreads();
+    for (int k = warp; k < G; k += nwarps) {
+        if (s_cur[k] >= 0) {
+            const float* src = job.llr + s_cur[k] * (long long)n;
+            for (int i = lane; i < n; i += 32) Ps[k * stride + i] = src[i];
+        }
+        if (s_next[k] >= 0) sp_prefetch(stage + k * nstage, job.llr, s_next[k], n, lane);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    __syncthreads();
+
+    auto comb = [](float a, float b) { return PROD ? __fmul_rn(a, b) : (a < b ? a : b); };
+    auto clampf = [maxv](float v) { return maxv < v ? maxv : v; };
+
+    for (int par = 0;; par ^= 1) {
+        // ================= one layered iteration =================
+        for (int l = 0; l < tb.L; ++l) {
+            if (active) {
+                const int d = tb.rw[l], eb = tb.ebase[l];
+                float q[DMAX], x[DMAX], f[DMAX];
+                int addr[DMAX];
+                uint32_t rx = 0;
+#pragma unroll
+                for (int j = 0; j < DMAX; ++j) {
+                    if (j < d) {
+                        const int e = eb + j;
+                        addr[j] = gbase + tb.colz[e] + sp_wrap(t, tb.shift[e], z);
+                        const float Q = __fsub_rn(Ps[addr[j]], Rt[e * nthr]);
+                        q[j] = Q;
+                        float a = __fsub_rn(fabsf(Q), beta);
+                        a = a > 0.0f ? a : 0.0f;
+                        x[j] = PROD ? lm_tanh(__fmul_rn(a, 0.5f)) : a;
+                        rx ^= __float_as_uint(Q);
+                    }
+                }
+                run_tree<DMAX>(d, x, f, comb, clampf);
+#pragma unroll
+                for (int j = 0; j < DMAX; ++j) {
+                    if (j < d) {
+                        const float fj = PROD ? __fmul_rn(2.0f, lm_atanh(f[j])) : f[j];
+                        const uint32_t sg = (rx ^ __float_as_uint(q[j])) & 0x80000000u;
+                        const float rn = __uint_as_float(__float_as_uint(fj) ^ sg);
+                        Ps[addr[j]] = __fadd_rn(q[j], rn);
+                        Rt[(eb + j) * nthr] = rn;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        if (tid == 0) { s_synd[par ^ 1] = 0; s_zero[par ^ 1] = 0; s_busy[par ^ 1] = 0; }
+
+        // ================= syndrome (early exit once this codeword fails) =================
+        if (active) {
+            for (int l = 0; l < tb.L; ++l) {
+                if (*reinterpret_cast<volatile uint32_t*>(&s_synd[par]) & (1u << g)) break;
+                const int d = tb.rw[l], eb = tb.ebase[l];
+                uint32_t xr = 0;
+                for (int j = 0; j < d; ++j) {
+                    const int e = eb + j;
+                    xr ^= __float_as_uint(Ps[gbase + tb.colz[e] + sp_wrap(t, tb.shift[e], z)]);
+                }
+                if (xr & 0x80000000u) {
+                    atomicOr(&s_synd[par], 1u << g);
+                    break;
+                }
+            }
+        }
+        __syncthreads();
+
+        // ====== each warp: its codewords -- decide, write out, promote, claim, prefetch ======
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncwarp();
+        for (int k = warp; k < G; k += nwarps) {
+            const long long cw = s_cur[k];
+            if (cw < 0) continue;
+            const int it = s_it[k] + 1;
+            const bool done = !(s_synd[par] & (1u << k)) || it >= job.max_iter;
+            if (!done) {
+                if (lane == 0) { s_it[k] = it; s_busy[par] = 1; }
+                continue;
+            }
+            const float* pk = Ps + k * stride;
+            const uint32_t* ref = job.ref_bits ? job.ref_bits + (cw % job.ref_period) * tb.hard_words : nullptr;
+            uint32_t mine = 0, refw = 0, errw = 0;
+            unsigned errslots = 0;
+            for (int w0 = 0; w0 < tb.hard_words; w0 += 32) {
+                if (ref && w0 + lane < tb.hard_words) refw = ref[w0 + lane];
+                const int wn = min(32, tb.hard_words - w0);
+                for (int w = 0; w < wn; ++w) {
+                    const int i = (w0 + w) * 32 + lane;
+                    const bool b = (i < tb.kbits) && (pk[i] < 0.0f);
+                    const uint32_t word = __ballot_sync(0xffffffffu, b);
+                    if (lane == w) mine = word;
+                    if (ref) {
+                        const uint32_t rw = __shfl_sync(0xffffffffu, refw, w);
+                        const bool er = (i < tb.kbits) && (b != (bool)((rw >> lane) & 1u));
+                        if (er) errslots |= 1u << ((i % z) % job.num_par);
+                        errw += __popc(__ballot_sync(0xffffffffu, er));
+                    }
+                }
+                if (job.hard_out && lane < wn) job.hard_out[cw * tb.hard_words + w0 + lane] = mine;
+            }
+            if (job.post_out) {
+                float* dst = job.post_out + cw * (long long)n;
+                for (int i = lane; i < n; i += 32) dst[i] = pk[i];
+            }
+            if (lane == 0 && job.iters_out) job.iters_out[cw] = (uint8_t)it;
+            if (job.counters) {
+                const unsigned slots = __reduce_or_sync(0xffffffffu, errslots);
+                if (lane == 0) {
+                    int bk = (int)(cw / job.bucket_size);
+                    bk = bk < job.n_buckets ? bk : job.n_buckets - 1;
+                    atomicAdd(&s_cnt[bk][0], 1ull);
+                    atomicAdd(&s_cnt[bk][1], (unsigned long long)it);
+                    if (errw) {
+                        atomicAdd(&s_cnt[bk][2], (unsigned long long)errw);
+                        atomicAdd(&s_cnt[bk][3], (unsigned long long)__popc(slots));
+                    }
+                }
+            }
+            __syncwarp();
+            const long long nxt = s_next[k];
+            if (nxt >= 0) {
+                const float* st = stage + k * nstage;
+                for (int i = lane; i < n; i += 32) Ps[k * stride + i] = st[i];
+                __syncwarp();
+                unsigned long long c = 0;
+                if (lane == 0) c = atomicAdd(&s_head, 1ull);
+                c = __shfl_sync(0xffffffffu, c, 0);
+                const long long fresh = (long long)c < hi ? (long long)c : -1;
+                if (fresh >= 0) sp_prefetch(stage + k * nstage, job.llr, fresh, n, lane);
+                if (lane == 0) { s_next[k] = fresh; s_busy[par] = 1; }
+            }
+            if (lane == 0) {
+                s_cur[k] = nxt;
+                s_it[k] = 0;
+                atomicOr(&s_zero[par], 1u << k);
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        __syncthreads();
+        if (active && (s_zero[par] & (1u << g)))
+            for (int e = 0; e < tb.E; ++e) Rt[e * nthr] = 0.f;
+        if (!s_busy[par]) break;
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    if (job.counters) {
+        __syncthreads();
+        for (int i = tid; i < job.n_buckets * 4; i += nthr) {
+            const unsigned long long v = (&s_cnt[0][0])[i];
+            if (v) atomicAdd(job.counters + i, v);
+        }
+    }
+}
+
+}  // namespace ldpc

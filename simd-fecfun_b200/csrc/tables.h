@@ -42,7 +42,8 @@ constexpr int SP_MAX_L = 64;
 constexpr int SP_MAX_E = 512;
 
 struct SpTables {
-    int z, mcol, n, L, G;            // G = codewords per CTA (one per lane group of Z threads)
+    int z, mcol, n, L, G;            // G = codewords per CTA (one per group of Z threads)
+    int stride;                      // posterior words per group in shared memory
     int kbits, hard_words;
     int E;                           // sum of row weights
     int16_t rw[SP_MAX_L];
@@ -67,7 +68,7 @@ struct SpJob {
     int prod;                        // 1 = sum-product, 0 = offset min-sum
     float beta;
     float maxv;                      // Max_val as decode_row computes it
-    unsigned long long* queue;
+    float* r_scratch;                // global check messages when they do not fit shared memory
 };
 
 // ---- fused generation ----
