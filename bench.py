@@ -49,7 +49,7 @@ def _clock_sampler(dev_index):
          "clocks_event_reasons.sw_power_cap")
     try:
         p = subprocess.Popen(["nvidia-smi", "-i", str(dev_index), "--query-gpu=" + q, "--format=csv,noheader,nounits",
-                              "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                              "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
     except OSError:
         return None
     return p
@@ -90,6 +90,23 @@ def _dist():
     return ws, rank, local
 
 
+class _quiet_stdout:
+    """Silence fd 1 (the reference's loaders print 'Matrix Params' lines;
+    bench.py must print exactly one JSON line)."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *a):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
 def cpu_reference_rate(llr_sample, threads, per_thread_cw, reps):
     """The reference's own LDPCdecode_set (oracle/_ref build, AVX-512) on host
     threads, one context per thread, decode-only time as the reference's RDTSC
@@ -100,7 +117,8 @@ def cpu_reference_rate(llr_sample, threads, per_thread_cw, reps):
     from ldpc_b200 import codes
     lib = rb.RefLib("Vec64c_min")
     code = codes.make_code(CODE)
-    ctxs = [rb.RefCtx(lib, code, per_thread_cw) for _ in range(threads)]
+    with _quiet_stdout():
+        ctxs = [rb.RefCtx(lib, code, per_thread_cw) for _ in range(threads)]
     saved = []
     for k, c in enumerate(ctxs):
         c.set_llr(llr_sample[k * per_thread_cw:(k + 1) * per_thread_cw])
@@ -150,7 +168,8 @@ def run_reference(args):
     # LDPCencode, gen_metrics), one SNR point per thread in rotation, untimed
     ctxs = []
     for k in range(threads):
-        c = rb.RefCtx(lib, code, per)
+        with _quiet_stdout():
+            c = rb.RefCtx(lib, code, per)
         seeds = (np.arange(64, dtype=np.uint64) + np.uint64(1000 + k)) * np.uint64(0x9E3779B97F4A7C15) | np.uint64(1)
         rb.ref_init_randstate(lib, seeds)
         wgn = rb.ref_normdist2(lib, c.wgn_count())
@@ -202,7 +221,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n-per-snr", type=int, default=1_000_000)
