@@ -206,6 +206,39 @@ int ldpc_simulate(ldpc_ctx *ctx, uint64_t seed, uint64_t cw_offset, const float 
 int ldpc_count_errors(ldpc_ctx *ctx, const uint32_t *hard, size_t n, const uint32_t *data_bits, size_t ref_period,
                       unsigned long long *counters, void *stream);
 
+/* ---- decoding without allocation --------------------------------------------
+ *
+ * No counterpart in the reference: the reference's decoder runs on the host
+ * and never touches device memory.
+ *
+ * Float decoding (LDPC_F32_SP / LDPC_F32_OMS) that allocates no device
+ * memory: no context is needed and nothing is allocated or freed, whatever
+ * the code.  It is for callers that cannot allocate at that point:
+ *   - their device memory is reserved up front by another allocator;
+ *   - cudaFree (and at times cudaMalloc) synchronising the device would stall
+ *     their other streams;
+ *   - they cannot handle an out-of-memory failure mid-run.
+ * ldpc_ctx_create, by contrast, allocates counters and tables, plus a message
+ * scratch of tens of MB for large codes.
+ *
+ * Check messages go to one static 32 MiB array per device, reserved when the
+ * library's kernels load there.
+ *   - The grid is capped at the number of CTAs the array holds.
+ *   - A code that needs more than the whole array for one CTA (edges per
+ *     lifted row block x CTA threads x 4 bytes) is rejected with
+ *     LDPC_ERR_UNSUPPORTED.
+ *   - Nothing in it needs to start at zero.
+ *
+ * Arguments and outputs are those of ldpc_decode_f32 (dev pointers, async on
+ * `stream`), on the CURRENT device; cfg's llr_scale / max_abs_llr are unused.
+ *
+ * The first call on each device does the setup: symbol lookup and kernel
+ * attributes.  Make it before any stream capture, from one thread.  Two calls
+ * whose kernels may overlap on the same device race on the shared array:
+ * order them (one stream, or events). */
+int ldpc_decode_f32_noalloc(const ldpc_code *code, const ldpc_cfg *cfg, const float *llr, size_t n,
+                            float *post_out, uint32_t *hard_out, uint8_t *iters_out, void *stream);
+
 /* ---- measurement ----------------------------------------------------------- */
 
 /* Sustained 32-bit integer instruction rate of `device` (ops/s), from a

@@ -77,6 +77,7 @@ _PROTOS = {
     "ldpc_count_errors": (C.c_int, [_vp, _vp, _sz, _vp, _sz, _vp, _vp]),
     "ldpc_decode_count": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _sz, _sz, _vp, C.c_int, _vp]),
     "ldpc_probe_int32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+    "ldpc_decode_f32_noalloc": (C.c_int, [_vp, C.POINTER(Cfg), _vp, _sz, _vp, _vp, _vp, _vp]),
 }
 
 if not os.path.exists(LIB_PATH):
