@@ -69,10 +69,13 @@ static void run_tree_f32(const int32_t *prog, int len, int d, int prod, const fl
  * the caller (same schedule) */
 static const orc_trees *g_trees_i8 = 0;
 
-int orc_decode_int8(const orc_code *c, const int8_t *llr, size_t n_cw, unsigned max_iter,
-                    float max_row_metric, float beta, int8_t *post_out, uint32_t *iters_out) {
+/* int8 layered offset min-sum with offset beta8[r] on layer r (the
+ * reference's decoder has one offset for every layer; per-layer offsets are
+ * the learned-offset extension). */
+int orc_decode_int8_layers(const orc_code *c, const int8_t *llr, size_t n_cw, unsigned max_iter,
+                           float max_row_metric, const int8_t *beta_layer, int8_t *post_out, uint32_t *iters_out) {
     const int z = c->z, n = z * c->mcol, E = total_edges(c), dmax = max_weight(c);
-    const int8_t beta8 = (int8_t)beta, maxv = max_row_i8(max_row_metric);
+    const int8_t maxv = max_row_i8(max_row_metric);
     int8_t *P = (int8_t *)malloc((size_t)n);
     int8_t *R = (int8_t *)malloc((size_t)E * z);
     int8_t *Q = (int8_t *)malloc((size_t)dmax), *m = (int8_t *)malloc((size_t)dmax);
@@ -87,6 +90,7 @@ int orc_decode_int8(const orc_code *c, const int8_t *llr, size_t n_cw, unsigned 
             int e0 = 0;
             for (int r = 0; r < c->mrow; ++r) {
                 const int d = c->row_weights[r];
+                const int8_t beta8 = beta_layer[r];
                 for (int t = 0; t < z; ++t) {
                     int8_t rx = 0;
                     for (int j = 0; j < d; ++j) {
@@ -135,6 +139,15 @@ int orc_decode_int8(const orc_code *c, const int8_t *llr, size_t n_cw, unsigned 
     }
     free(P); free(R); free(Q); free(m); free(f); free(node); free(v);
     return 0;
+}
+
+int orc_decode_int8(const orc_code *c, const int8_t *llr, size_t n_cw, unsigned max_iter,
+                    float max_row_metric, float beta, int8_t *post_out, uint32_t *iters_out) {
+    int8_t *b = (int8_t *)malloc((size_t)(c->mrow > 0 ? c->mrow : 1));
+    for (int r = 0; r < c->mrow; ++r) b[r] = (int8_t)beta;   /* implicit float -> int truncation, decode_functions.cpp:60 */
+    const int rc = orc_decode_int8_layers(c, llr, n_cw, max_iter, max_row_metric, b, post_out, iters_out);
+    free(b);
+    return rc;
 }
 
 static uint32_t fbits(float x) { uint32_t u; memcpy(&u, &x, 4); return u; }

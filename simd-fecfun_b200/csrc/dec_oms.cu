@@ -78,6 +78,8 @@ bool matches(const OmsInst& in, const ldpc_code& c) {
 int setup_oms(ldpc_ctx* x) {
     const ldpc_code& c = x->code;
     const int L = c.mrow;
+    // LDPC_OMS_RT forces the run-time-table kernel (tuning and cross-checks)
+    if (getenv("LDPC_OMS_RT")) return setup_oms_rt(x);
     const OmsInst* best = nullptr;
     const bool use_compiled = !getenv("LDPC_OMS_NO_COMPILED");
     const bool use_split = !getenv("LDPC_OMS_NO_SPLIT");
@@ -86,11 +88,8 @@ int setup_oms(ldpc_ctx* x) {
         if (in.rw) { best = &in; break; }
         if (!best || in.D < best->D) best = &in;
     }
-    if (!best)
-        return fail(LDPC_ERR_UNSUPPORTED, "int8 decoder: no kernel for %d layers of weight <= %d (Z=%d)", L,
-                    c.max_row_weight, c.z);
-    if (L > OMS_MAX_L || L * best->D > OMS_MAX_SLOTS_E)
-        return fail(LDPC_ERR_UNSUPPORTED, "int8 decoder: %d layers x %d edge slots exceed the parameter block", L, best->D);
+    // shapes without a register-resident instantiation: run-time tables
+    if (!best || L > OMS_MAX_L || L * best->D > OMS_MAX_SLOTS_E || c.z > 640) return setup_oms_rt(x);
     x->inst = best;
     OmsTables& t = x->omst;
     memset(&t, 0, sizeof(t));
@@ -157,6 +156,7 @@ int setup_oms(ldpc_ctx* x) {
 }
 
 int launch_oms(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s) {
+    if (x->oms_rt) return launch_oms_rt(x, a, s);
     if (!x->inst) return fail(LDPC_ERR_INVALID_ARG, "context was not created for the int8 decoder");
     if (a.n == 0) return LDPC_OK;
     if (a.queue < 0 || a.queue >= ldpc_ctx::kQueues) return fail(LDPC_ERR_INVALID_ARG, "queue %d", a.queue);

@@ -66,7 +66,8 @@ int setup_sp(ldpc_ctx* x) {
         if (k.dmax == dmax && k.prod == prod && k.rsmem == rsmem) v = &k;
     x->sp_kernel = v->k;
     x->sp_smem = (int)(base_smem + (rsmem ? r_smem : 0));
-    if (x->sp_smem > 200 * 1024) return fail(LDPC_ERR_UNSUPPORTED, "float decoder: %d B of shared memory", x->sp_smem);
+    // up to 220 KB dynamic (B200: 227 KB per CTA, less the kernel's static shared memory)
+    if (x->sp_smem > 220 * 1024) return fail(LDPC_ERR_UNSUPPORTED, "float decoder: %d B of shared memory", x->sp_smem);
     CUDA_TRY(cudaFuncSetAttribute((const void*)v->k, cudaFuncAttributeMaxDynamicSharedMemorySize, x->sp_smem));
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)v->k, x->sp_threads, x->sp_smem));

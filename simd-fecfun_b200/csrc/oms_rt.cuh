@@ -1,0 +1,283 @@
+// Layered int8 offset min-sum over run-time code tables: any code shape
+// (802.11ay, 802.3ca, 5G NR base graphs 1 and 2, ...) and several codes in one
+// launch.  Same arithmetic as oms_f16_kernel (packed f16x2 lanes, two
+// codewords per 32-bit word, reference int8 semantics bit for bit:
+// decode_functions.cpp:11-103, LDPCdecode.cpp:79-201), with
+//   - the layer loop over tables in shared memory (row weights, edge columns
+//     and shifts), unrolled to DMAX edge slots per layer;
+//   - the offset beta8 per layer (a single beta is the reference's case; a
+//     table of per-layer offsets serves learned offsets);
+//   - the check messages in shared memory (RSMEM) or, for large codes, in a
+//     per-CTA global scratch area (L2-resident at these sizes);
+//   - work given as chunks (a job's codeword range): CTA b decodes chunks
+//     b, b + grid, ...; within a chunk the persistent slot refill of
+//     oms_f16_kernel keeps every slot busy.
+#pragma once
+#include "oms_f16.cuh"
+
+namespace ldpc {
+
+template <int DMAX, bool QUIRK>
+__device__ __forceinline__ void rt_layer(const RtCode& C, int l, uint32_t* Ps, uint32_t* Rt, int nthr, int t, int gbase,
+                                         int z) {
+    constexpr uint32_t SGN = 0x80008000u;
+    const int d = C.rw[l], eb = C.ebase[l];
+    const uint32_t beta2 = C.beta2[l];
+    const uint32_t quirk = QUIRK ? C.quirk2[l] : 0u;
+    uint32_t q[DMAX];
+    int addr[DMAX];
+    uint32_t mn1 = H2_1024, mn2 = H2_1024;
+    uint32_t sx = 0;
+#pragma unroll
+    for (int j = 0; j < DMAX; ++j) {
+        if (j < d) {
+            const uint32_t ed = C.edge[eb + j];
+            addr[j] = gbase + (int)(ed >> 9) + wrap_add(t, (int)(ed & 511u), z);
+            uint32_t Q = hsub2(Ps[addr[j]], Rt[(eb + j) * nthr]);
+            Q = hmin2(hmax2(Q, H2_M128), H2_P127);
+            uint32_t a = habs2(Q);
+            if (QUIRK) a = hfma2(heq2(Q, H2_M128), quirk, a);
+            mn2 = hmin2(mn2, hmax2(mn1, a));
+            mn1 = hmin2(mn1, a);
+            q[j] = Q;
+            sx ^= Q;
+        }
+    }
+    const uint32_t c1 = hmin2(hmax2(hsub2(mn1, beta2), H2_ZERO), C.maxv2);
+    const uint32_t c2 = hmin2(hmax2(hsub2(mn2, beta2), H2_ZERO), C.maxv2);
+    const uint32_t X = c1 ^ c2;
+    const uint32_t M1 = c1 ^ (sx & SGN);
+#pragma unroll
+    for (int j = 0; j < DMAX; ++j) {
+        if (j < d) {
+            uint32_t a = habs2(q[j]);
+            if (QUIRK) a = hfma2(heq2(q[j], H2_M128), quirk, a);
+            const uint32_t eq = heq2_mask(a, mn1);
+            const uint32_t Rn = M1 ^ (q[j] & SGN) ^ (eq & X);
+            const uint32_t Pn = hmin2(hmax2(hadd2(q[j], Rn), H2_M128), H2_P127);
+            Ps[addr[j]] = Pn;
+            Rt[(eb + j) * nthr] = Rn;
+        }
+    }
+}
+
+// syndrome of this thread's check rows with early exit (as oms_syndrome)
+template <int DMAX>
+__device__ __forceinline__ void rt_syndrome(const RtCode& C, const uint32_t* Ps, int t, int gbase, int z, uint32_t* synd) {
+    uint32_t seen = 0;
+    for (int l = 0; l < C.L; ++l) {
+        const int d = C.rw[l], eb = C.ebase[l];
+        uint32_t x = 0;
+#pragma unroll
+        for (int j = 0; j < DMAX; ++j) {
+            if (j < d) {
+                const uint32_t ed = C.edge[eb + j];
+                x ^= Ps[gbase + (int)(ed >> 9) + wrap_add(t, (int)(ed & 511u), z)];
+            }
+        }
+        x &= 0x80008000u;
+        if (x & ~seen) {
+            atomicOr(synd, x);
+            seen |= x;
+        }
+        if (((seen | *reinterpret_cast<volatile uint32_t*>(synd)) & 0x80008000u) == 0x80008000u) break;
+    }
+}
+
+// Shared memory: [RtCode copy][posteriors G x stride words][LLR staging 2G x nstage bytes][messages E x blockDim words if RSMEM]
+__host__ __device__ constexpr int rt_code_bytes() { return (int)((sizeof(RtCode) + 15) & ~(size_t)15); }
+
+template <int DMAX, bool QUIRK, bool RSMEM>
+__global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtLaunch lp) {
+    extern __shared__ __align__(16) unsigned char rt_smem[];
+    __shared__ long long s_cur[32];
+    __shared__ long long s_next[32];
+    __shared__ int s_it[32];
+    __shared__ uint32_t s_synd[2][16];
+    __shared__ uint32_t s_zero_mask[2][16];
+    __shared__ int s_busy[2];
+    __shared__ unsigned long long s_head;
+    __shared__ unsigned long long s_cnt[OMS_MAX_BUCKETS][4];
+    __shared__ int s_code_idx;
+
+    const RtCode& C = *reinterpret_cast<const RtCode*>(rt_smem);
+    uint32_t* const Ps = reinterpret_cast<uint32_t*>(rt_smem + rt_code_bytes());
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int warp = tid >> 5, lane = tid & 31, nwarps = nthr >> 5;
+    if (tid == 0) s_code_idx = -1;
+
+    const int n_chunks = lp.jobs ? lp.n_chunks : (int)gridDim.x;
+    for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
+        // ---------------- chunk set-up ----------------
+        RtJob job;
+        long long lo, hi;
+        if (lp.jobs) {
+            const RtChunk ch = lp.chunks[ci];
+            job = lp.jobs[ch.job];
+            lo = ch.lo;
+            hi = ch.hi;
+        } else {
+            job = lp.job0;
+            lo = job.ncw * ci / gridDim.x;
+            hi = job.ncw * (ci + 1) / gridDim.x;
+        }
+        __syncthreads();   // the previous chunk is finished with the shared tables
+        if (s_code_idx != job.code) {
+            const uint4* src = reinterpret_cast<const uint4*>(lp.codes + job.code);
+            uint4* dst = reinterpret_cast<uint4*>(rt_smem);
+            for (int i = tid; i < (int)(sizeof(RtCode) / 16); i += nthr) dst[i] = src[i];
+            __syncthreads();
+            if (tid == 0) s_code_idx = job.code;
+        }
+        const int z = C.z, n = C.n, G = C.G, stride = C.stride, E = C.E;
+        const int nslots = 2 * G;
+        const int nstage = (n + 15) & ~15;
+        int8_t* const stage_base = reinterpret_cast<int8_t*>(Ps) + ((G * stride * 4 + 15) & ~15);
+        const int t = tid / G, g = tid - (tid / G) * G;
+        const bool active = t < z;
+        const int gbase = g * stride;
+        uint32_t* const Rt = RSMEM ? reinterpret_cast<uint32_t*>(stage_base + 2 * G * nstage) + tid
+                                   : lp.r_scratch + (long long)blockIdx.x * lp.r_words_per_cta + tid;
+
+        for (int i = tid; i < OMS_MAX_BUCKETS * 4; i += nthr) (&s_cnt[0][0])[i] = 0;
+        for (int i = tid; i < G * stride; i += nthr) Ps[i] = 0;
+        for (int e = 0; e < E; ++e) Rt[e * nthr] = 0u;
+        if (tid < 32) {
+            const long long c0 = lo + tid, c1 = lo + nslots + tid;
+            const bool ok = tid < nslots;
+            s_cur[tid] = ok && c0 < hi ? c0 : -1;
+            s_next[tid] = ok && c1 < hi ? c1 : -1;
+            s_it[tid] = 0;
+            if (tid < 16) {
+                s_synd[0][tid] = s_synd[1][tid] = 0;
+                s_zero_mask[0][tid] = s_zero_mask[1][tid] = 0;
+            }
+            if (tid < 2) s_busy[tid] = 0;
+        }
+        if (tid == 0) s_head = (unsigned long long)(lo + 2 * nslots);
+        __syncthreads();
+        for (int k = warp; k < nslots; k += nwarps) {
+            const long long cw = s_cur[k];
+            if (cw >= 0) {
+                __half* dst = reinterpret_cast<__half*>(Ps + (k >> 1) * stride) + (k & 1);
+                const int8_t* src = job.llr + cw * (long long)n;
+                for (int i = lane; i < n; i += 32) dst[2 * i] = __int2half_rn((int)src[i]);
+            }
+            if (s_next[k] >= 0) prefetch_llr(stage_base + k * nstage, job.llr, s_next[k], n, lane);
+        }
+        cp_async_commit();
+        __syncthreads();
+
+        for (int par = 0;; par ^= 1) {
+            // ---------------- one layered iteration ----------------
+            for (int l = 0; l < C.L; ++l) {
+                if (active) rt_layer<DMAX, QUIRK>(C, l, Ps, Rt, nthr, t, gbase, z);
+                __syncthreads();
+            }
+            if (tid < 16) {
+                s_synd[par ^ 1][tid] = 0;
+                s_zero_mask[par ^ 1][tid] = 0;
+            }
+            if (tid == 0) s_busy[par ^ 1] = 0;
+            if (active) rt_syndrome<DMAX>(C, Ps, t, gbase, z, &s_synd[par][g]);
+            __syncthreads();
+
+            // ------- each warp: its slots -- decide, write out, promote, claim, prefetch -------
+            cp_async_wait_all();
+            __syncwarp();
+            for (int k = warp; k < nslots; k += nwarps) {
+                const long long cw = s_cur[k];
+                if (cw < 0) continue;
+                const int gg = k >> 1, hsel = k & 1;
+                const int it = s_it[k] + 1;
+                const uint32_t bit = hsel ? 0x80000000u : 0x00008000u;
+                const bool done = !(s_synd[par][gg] & bit) || it >= C.max_iter;
+                if (!done) {
+                    if (lane == 0) {
+                        s_it[k] = it;
+                        s_busy[par] = 1;
+                    }
+                    continue;
+                }
+                __half* pk = reinterpret_cast<__half*>(Ps + gg * stride) + hsel;
+                const uint32_t* ref = job.ref_bits ? job.ref_bits + (cw % job.ref_period) * C.hard_words : nullptr;
+                uint32_t mine = 0, refw = 0, errw = 0;
+                unsigned errslots = 0;
+                for (int w0 = 0; w0 < C.hard_words; w0 += 32) {
+                    if (ref && w0 + lane < C.hard_words) refw = ref[w0 + lane];
+                    const int wn = min(32, C.hard_words - w0);
+                    for (int w = 0; w < wn; ++w) {
+                        const int i = (w0 + w) * 32 + lane;
+                        const bool b = (i < C.kbits) && __hlt(pk[2 * i], __float2half(0.0f));
+                        const uint32_t word = __ballot_sync(0xffffffffu, b);
+                        if (lane == w) mine = word;
+                        if (ref) {
+                            const uint32_t rw = __shfl_sync(0xffffffffu, refw, w);
+                            const bool e = (i < C.kbits) && (b != (bool)((rw >> lane) & 1u));
+                            if (e) errslots |= 1u << ((i % z) % C.num_par);
+                            errw += __popc(__ballot_sync(0xffffffffu, e));
+                        }
+                    }
+                    if (job.hard_out && lane < wn) job.hard_out[cw * C.hard_words + w0 + lane] = mine;
+                }
+                if (job.post_out) {
+                    int8_t* dst = job.post_out + cw * (long long)n;
+                    for (int i = lane; i < n; i += 32) dst[i] = (int8_t)__half2int_rn(pk[2 * i]);
+                }
+                if (lane == 0 && job.iters_out) job.iters_out[cw] = (uint8_t)it;
+                if (job.counters) {
+                    const unsigned slots = __reduce_or_sync(0xffffffffu, errslots);
+                    if (lane == 0) {
+                        int bk = (int)(cw / job.bucket_size);
+                        bk = bk < job.n_buckets ? bk : job.n_buckets - 1;
+                        atomicAdd(&s_cnt[bk][0], 1ull);
+                        atomicAdd(&s_cnt[bk][1], (unsigned long long)it);
+                        if (errw) {
+                            atomicAdd(&s_cnt[bk][2], (unsigned long long)errw);
+                            atomicAdd(&s_cnt[bk][3], (unsigned long long)__popc(slots));
+                        }
+                    }
+                }
+                __syncwarp();
+                const long long nxt = s_next[k];
+                if (nxt >= 0) {
+                    const int8_t* st = stage_base + k * nstage;
+                    for (int i = lane; i < n; i += 32) pk[2 * i] = __int2half_rn((int)st[i]);
+                    __syncwarp();
+                    unsigned long long c = 0;
+                    if (lane == 0) c = atomicAdd(&s_head, 1ull);
+                    c = __shfl_sync(0xffffffffu, c, 0);
+                    const long long fresh = (long long)c < hi ? (long long)c : -1;
+                    if (fresh >= 0) prefetch_llr(stage_base + k * nstage, job.llr, fresh, n, lane);
+                    if (lane == 0) {
+                        s_next[k] = fresh;
+                        s_busy[par] = 1;
+                    }
+                }
+                if (lane == 0) {
+                    s_cur[k] = nxt;
+                    s_it[k] = 0;
+                    atomicOr(&s_zero_mask[par][gg], hsel ? 0xffff0000u : 0x0000ffffu);
+                }
+            }
+            cp_async_commit();
+            __syncthreads();
+            if (active) {
+                const uint32_t m = s_zero_mask[par][g];
+                if (m)
+                    for (int e = 0; e < E; ++e) Rt[e * nthr] &= ~m;
+            }
+            if (!s_busy[par]) break;
+        }
+        cp_async_wait_all();
+        if (job.counters) {
+            __syncthreads();
+            for (int i = tid; i < job.n_buckets * 4; i += nthr) {
+                const unsigned long long v = (&s_cnt[0][0])[i];
+                if (v) atomicAdd(job.counters + i, v);
+            }
+        }
+    }
+}
+
+}  // namespace ldpc

@@ -71,6 +71,58 @@ struct SpJob {
     float* r_scratch;                // global check messages when they do not fit shared memory
 };
 
+// ---- int8 offset min-sum with run-time code tables (any shape; several codes per launch) ----
+constexpr int RT_MAX_L = 64;
+constexpr int RT_MAX_E = 1024;
+constexpr int RT_MAX_Z = 511;        // shifts are packed in 9 bits
+
+// One code of a launch, in device memory; a CTA copies it into shared memory
+// when it starts work on that code.
+struct alignas(16) RtCode {
+    int z, n, L, E;
+    int G;                           // codeword pairs per CTA (thread (t, g): check row t, pair g)
+    int stride;                      // posterior words per pair in shared memory
+    int kbits, hard_words, num_par, max_iter;
+    uint32_t maxv2;                  // half2 bits of Max8
+    uint32_t beta2[RT_MAX_L];        // half2 bits of beta8 per layer
+    uint32_t quirk2[RT_MAX_L];       // -128.0 in both lanes where beta8 = 0 (abs8(-128) = -128), else 0
+    int16_t rw[RT_MAX_L];
+    int16_t ebase[RT_MAX_L];         // first edge of layer l
+    uint32_t edge[RT_MAX_E];         // (column * Z) << 9 | shift
+};
+
+// One batch of codewords of one code (device pointers).
+struct RtJob {
+    const int8_t* llr;               // [ncw][n]
+    long long ncw;
+    int8_t* post_out;
+    uint32_t* hard_out;
+    uint8_t* iters_out;
+    const uint32_t* ref_bits;
+    long long ref_period;
+    long long bucket_size;
+    unsigned long long* counters;    // [n_buckets][4] as OmsJob
+    int n_buckets;
+    int code;                        // index into the launch's code array
+};
+
+// Codewords [lo, hi) of job `job`, decoded by one CTA.
+struct RtChunk {
+    int job;
+    int pad;
+    long long lo, hi;
+};
+
+struct RtLaunch {
+    const RtCode* codes;
+    const RtJob* jobs;               // null: one job, job0, split evenly over the grid
+    const RtChunk* chunks;           // CTA b takes chunks b, b + grid, b + 2 grid, ...
+    int n_chunks;
+    RtJob job0;
+    uint32_t* r_scratch;             // check messages in global memory (when not in shared memory)
+    long long r_words_per_cta;
+};
+
 // ---- fused generation ----
 constexpr int GEN_MAX_TERMS = 1024;
 constexpr int GEN_MAX_PAR = 64;

@@ -23,6 +23,7 @@ All shifts follow the reference's rule "shift mod Z" (ExpandH.m:14 uses
 from __future__ import annotations
 
 import json
+import re
 import os
 import struct
 from dataclasses import dataclass, field
@@ -191,11 +192,20 @@ def _gen_encode(hc, z, direct_cols, subst_row, subst_col, punc_list, fill_list):
     col_cnts: List[int] = []
     par_offset: List[int] = []
     if direct_cols:
-        h = expand_h(hc, z)
-        k = h.shape[1] - h.shape[0]
-        m1, m2 = h[:, :k], h[:, k:]
+        # Rows z*(d-1) of inv(M2) M1.  When the parity part is block lower
+        # triangular, M2 = [[A, 0], [C, D]] with A the leading m0 x m0 base
+        # blocks (5G NR: the 4 x 4 core), those rows of inv(M2) are rows of
+        # inv(A) padded with zeros, so only A and the first m0 block rows of
+        # M1 are expanded.
+        kb = mcol - mrow
+        par = hc[:, kb:]
+        m0 = max(direct_cols)
+        while m0 < mrow and (par[:m0, m0:] >= 0).any():
+            m0 += 1
+        a = expand_h(par[:m0, :m0], z)
+        m1 = expand_h(hc[:m0, :kb], z)
         want = [z * (d - 1) for d in direct_cols]
-        inv_rows = _gf2_solve_rows(m2, want)
+        inv_rows = _gf2_solve_rows(a, want)
         row1_direct = (inv_rows.astype(np.int64) @ m1.astype(np.int64)) % 2
         for ii in range(len(direct_cols)):
             idx = np.nonzero(row1_direct[ii])[0]
@@ -365,6 +375,20 @@ class Code:
     def full_h(self) -> np.ndarray:
         return expand_h(self.hc, self.z)
 
+    def syndrome(self, cw: np.ndarray) -> np.ndarray:
+        """H c over GF(2) for codewords cw [n][N] (0/1), without expanding H:
+        check t of row block r sums bit (t + s) % Z of every column block c
+        with shift s = hc[r, c] (ExpandH.m's circulant).  Returns [n][mrow*Z]."""
+        cw = np.asarray(cw, dtype=np.uint8).reshape(-1, self.n)
+        z = self.z
+        out = np.zeros((cw.shape[0], self.mrow * z), np.uint8)
+        idx = np.arange(z)
+        for r in range(self.mrow):
+            acc = out[:, r * z:(r + 1) * z]
+            for c in np.nonzero(self.hc[r] >= 0)[0]:
+                acc ^= cw[:, c * z + (idx + int(self.hc[r, c])) % z]
+        return out
+
 
 def make_code(name: str, num_par: int = 1, z_over: Optional[int] = None,
               simd_size: int = 512, elem_size: int = 8) -> Code:
@@ -380,6 +404,99 @@ def make_code(name: str, num_par: int = 1, z_over: Optional[int] = None,
     if z_over is not None:
         z = int(z_over)
     return _build(name, hc, z, num_par, direct, srow, scol, [], [], simd_size // elem_size)
+
+
+# ----------------------------------------------------------------------------
+# 5G NR codes (GetHMatrix.m:398-434 for '5GNR_n<#>_k<#>', with the lifting
+# size rules of 3GPP TS 38.212 restated for Hbg_fill_puncture(n, k), which the
+# reference calls but does not ship)
+# ----------------------------------------------------------------------------
+
+# TS 38.212 Table 5.3.2-1: set index iLS holds the lifting sizes a * 2^j <= 384
+NR_LIFT_A = (2, 3, 5, 7, 9, 11, 13, 15)
+NR_INFO_COLS = {1: 22, 2: 10}          # systematic base columns (2 of them punctured)
+NR_ROWS = {1: 46, 2: 42}
+NR_MAX_K = {1: 22 * 384, 2: 10 * 384}
+
+
+def nr_lifting_sizes() -> Dict[int, int]:
+    """Every 5G NR lifting size Z with its set index iLS."""
+    out = {}
+    for ils, a in enumerate(NR_LIFT_A):
+        z = a
+        while z <= 384:
+            out[z] = ils
+            z *= 2
+    return dict(sorted(out.items()))
+
+
+def nr_select(n: int, k: int) -> Tuple[int, int, int]:
+    """(base graph, Z, iLS) for k information bits sent as n code bits.
+    Base graph per TS 38.212 7.2.2 (graph 2 if k <= 292, or k <= 3824 and
+    k/n <= 0.67, or k/n <= 0.25); Kb = 22 for graph 1, else 10/9/8/6 for
+    k > 640 / > 560 / > 192 / otherwise (5.2.2); Z = the smallest lifting size
+    with Kb * Z >= k."""
+    if not (0 < k < n):
+        raise ValueError("need 0 < k < n")
+    r = k / n
+    bg = 2 if (k <= 292 or (k <= 3824 and r <= 0.67) or r <= 0.25) else 1
+    kb = 22 if bg == 1 else (10 if k > 640 else 9 if k > 560 else 8 if k > 192 else 6)
+    sizes = nr_lifting_sizes()
+    cand = [z for z in sizes if kb * z >= k]
+    if not cand or k > NR_MAX_K[bg]:
+        raise ValueError("k=%d needs code block segmentation (base graph %d holds %d)" % (k, bg, NR_MAX_K[bg]))
+    z = cand[0]
+    return bg, z, sizes[z]
+
+
+def make_nr_code(n: int, k: int, num_par: int = 1, bg: Optional[int] = None, z: Optional[int] = None,
+                 simd_size: int = 512, elem_size: int = 8) -> Code:
+    """The reference's '5GNR_n<n>_k<k>' MatrixSet (GetHMatrix.m:398-434,
+    encode_method.m:185-190, gen_structs.m:29-39).  The first 2Z systematic
+    bits are punctured, parity bits beyond n are punctured at the end, and the
+    Z*Kb - k filler bits end the systematic part.  ``bg``/``z`` override the
+    TS 38.212 selection (e.g. to pick one lifting size of a set)."""
+    sel_bg, sel_z, _ = nr_select(n, k)
+    bg = sel_bg if bg is None else bg
+    z = sel_z if z is None else z
+    sizes = nr_lifting_sizes()
+    if z not in sizes:
+        raise ValueError("Z=%d is not a 5G NR lifting size" % z)
+    ils = sizes[z]
+    info_mcol = NR_INFO_COLS[bg]
+    if k > info_mcol * z:
+        raise ValueError("k=%d exceeds %d systematic columns of Z=%d" % (k, info_mcol, z))
+    start_punc = 2
+    p_mcol = -(-(n - k) // z) + start_punc
+    if not 4 <= p_mcol <= NR_ROWS[bg]:
+        raise ValueError("n=%d, k=%d needs %d parity columns (4..%d)" % (n, k, p_mcol, NR_ROWS[bg]))
+    h = nr_base_graph(bg, ils)[:p_mcol, :p_mcol + info_mcol]
+    h = np.where(h >= 0, h % z, -1)
+    mcol = p_mcol + info_mcol
+    punc_parity = z * (p_mcol - start_punc) - (n - k)
+    punc = [1, start_punc * z]
+    if punc_parity > 0:
+        punc += [z * mcol - punc_parity + 1, z * mcol]
+    fill_cnt = z * info_mcol - k
+    fill = [z * info_mcol - fill_cnt + 1, z * info_mcol] if fill_cnt > 0 else []
+    # gen_structs.m:33-37: scale the inclusive 1-based pairs by num_par, make them 0-based
+    scale = lambda lst: [((v - 1) * num_par + 1 if i % 2 == 0 else v * num_par) - 1 for i, v in enumerate(lst)]
+    srow = ([2, 4] + list(range(5, 100)))[:p_mcol - 2]
+    direct = [1, 3]
+    zz = z * num_par
+    hc = np.where(h >= 0, h * num_par, -1)
+    return _build("5GNR_n%d_k%d" % (n, k), hc, zz, num_par, direct, srow, list(srow), scale(punc), scale(fill),
+                  simd_size // elem_size)
+
+
+def code_by_name(name: str, **kw) -> Code:
+    """make_code for the named MatrixSets, make_nr_code for '5GNR_n<n>_k<k>'."""
+    if name.startswith("5GNR_"):
+        m = re.fullmatch(r"5GNR_n(\d+)_k(\d+)", name)
+        if not m:
+            raise KeyError("bad 5G NR MatrixSet %r (want 5GNR_n<n>_k<k>)" % name)
+        return make_nr_code(int(m.group(1)), int(m.group(2)), **kw)
+    return make_code(name, **kw)
 
 
 def _build(name, hc, z, num_par, direct, srow, scol, punc_list, fill_list, eps):

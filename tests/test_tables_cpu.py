@@ -106,3 +106,61 @@ def test_tree_min_equals_exclusive_minimum():
                     node[op[1]] = min(mx, node[op[1]])
             for j in range(d):
                 assert node[outs[j]] == min([mx] + [x[k] for k in range(d) if k != j])
+
+
+def test_nr_lifting_size_selection():
+    """TS 38.212 lifting sets (51 sizes) and the base-graph / Z choice for the
+    5G NR workloads: graph 1 Z=384 (k=8448) and graph 2 Z=64/128/256."""
+    from ldpc_b200 import codes
+    sizes = codes.nr_lifting_sizes()
+    assert len(sizes) == 51 and max(sizes) == 384 and sizes[384] == 1 and sizes[256] == 0 and sizes[15] == 7
+    assert codes.nr_select(25344, 8448) == (1, 384, 1)
+    assert codes.nr_select(6400, 1280) == (2, 128, 0)
+    assert codes.nr_select(12800, 2560) == (2, 256, 0)
+    assert codes.nr_select(3136, 576) == (2, 64, 0)     # Kb = 9: 9*60 < 576 <= 9*64
+    assert codes.nr_select(300, 100) == (2, 18, 4)      # Kb = 6
+    with pytest.raises(ValueError):
+        codes.nr_select(30000, 9000)                     # needs code block segmentation
+
+
+@pytest.mark.parametrize("name,mrow,mcol,punc,fill", [
+    ("5GNR_n25344_k8448", 46, 68, [0, 767], []),
+    ("5GNR_n3136_k576", 42, 52, [0, 127], [576, 639]),
+    ("5GNR_n1000_k500", 10, 20, [0, 127, 1268, 1279], [500, 639]),
+    ("5GNR_n10000_k8000", 8, 30, [0, 767, 11216, 11519], [8000, 8447]),
+])
+def test_nr_codes_encode_to_codewords(oracle, name, mrow, mcol, punc, fill):
+    """GetHMatrix's 5GNR_n<n>_k<k>: shape, puncture/filler lists, and H c = 0
+    for the encoder schedule (direct parity columns 1 and 3, then substitution)."""
+    from ldpc_b200 import codes
+    c = codes.code_by_name(name)
+    assert (c.mrow, c.mcol, c.punc_list, c.fill_list) == (mrow, mcol, punc, fill)
+    sent = c.n - c.punc_cnt_bits - c.fill_cnt          # punctured and filler bits are not sent
+    n_req, k_req = (int(v) for v in name[6:].split("_k"))
+    assert sent == n_req and c.k == k_req
+    rng = np.random.default_rng(2)
+    info = rng.integers(0, 2, (6, (c.mcol - c.mrow) * c.z), dtype=np.uint8)
+    for s, e in zip(c.fill_list[0::2], c.fill_list[1::2]):
+        info[:, s:e + 1] = 0
+    cw = oracle.encode(c, info)
+    assert np.array_equal(cw[:, :info.shape[1]], info)
+    assert not c.syndrome(cw).any()
+
+
+def test_nr_num_par_scales_lists():
+    """gen_structs.m:33-37: each puncture/filler pair scales by num_par."""
+    from ldpc_b200 import codes
+    a = codes.make_nr_code(1000, 500)
+    b = codes.make_nr_code(1000, 500, num_par=2)
+    assert b.z == 2 * a.z
+    assert b.punc_list == [a.punc_list[0] * 2, (a.punc_list[1] + 1) * 2 - 1, a.punc_list[2] * 2, (a.punc_list[3] + 1) * 2 - 1]
+    assert b.fill_list == [a.fill_list[0] * 2, (a.fill_list[1] + 1) * 2 - 1]
+
+
+def test_syndrome_matches_expanded_h(oracle):
+    from ldpc_b200 import codes
+    c = codes.make_code("16e 1/2")
+    rng = np.random.default_rng(5)
+    x = rng.integers(0, 2, (3, c.n), dtype=np.uint8)
+    want = (x.astype(np.int64) @ c.full_h().astype(np.int64).T) % 2
+    assert np.array_equal(c.syndrome(x), want.astype(np.uint8))
