@@ -243,7 +243,7 @@ void ldpc_code_destroy(ldpc_code* c) { delete c; }
 // ---------------------------------------------------------------------------
 // contexts
 // ---------------------------------------------------------------------------
-namespace {
+namespace ldpc {
 
 int8_t max_row_i8(float m) {
     // decode_row's Max_row_simd for an int8 build (decode_functions.cpp:27-32)
@@ -251,7 +251,7 @@ int8_t max_row_i8(float m) {
     return (int8_t)m;
 }
 
-}  // namespace
+}  // namespace ldpc
 
 extern "C" {
 
@@ -268,7 +268,10 @@ int ldpc_ctx_create(const ldpc_code* code, const ldpc_cfg* cfg, int device, ldpc
         return fail(LDPC_ERR_CUDA, "no CUDA device available");
     }
     if (device < 0 || device >= ndev) return fail(LDPC_ERR_INVALID_ARG, "device %d of %d", device, ndev);
-    std::unique_ptr<ldpc_ctx> x(new ldpc_ctx);
+    struct Destroy {
+        void operator()(ldpc_ctx* p) const { ldpc_ctx_destroy(p); }
+    };
+    std::unique_ptr<ldpc_ctx, Destroy> x(new ldpc_ctx);   // a failed set-up frees what it allocated
     x->code = *code;
     x->cfg = *cfg;
     x->device = device;
@@ -283,7 +286,7 @@ int ldpc_ctx_create(const ldpc_code* code, const ldpc_cfg* cfg, int device, ldpc
         if (!(cfg->max_row_metric > -128.0f && cfg->max_row_metric < 128.0f))
             return fail(LDPC_ERR_UNSUPPORTED, "int8 decoder: max_row_metric=%g outside int8", cfg->max_row_metric);
         const int beta8 = (int8_t)cfg->beta;
-        const int max8 = max_row_i8(cfg->max_row_metric);
+        const int max8 = ldpc::max_row_i8(cfg->max_row_metric);
         if (max8 < 0) return fail(LDPC_ERR_UNSUPPORTED, "int8 decoder: negative row clamp %d", max8);
         x->beta0 = beta8 == 0;
         x->beta2 = ldpc::half2_bits((float)beta8);
@@ -318,6 +321,8 @@ void ldpc_ctx_destroy(ldpc_ctx* x) {
     cudaFree(x->d_status);
     cudaFree(x->d_counters);
     cudaFree(x->d_sp_scratch);
+    cudaFree(x->d_rt_code);
+    cudaFree(x->d_rt_scratch);
     for (int i = 0; i < 2; ++i) {
         if (x->streams[i]) cudaStreamDestroy(x->streams[i]);
         for (int k = 0; k < 4; ++k) cudaFree(x->d_pipe[i][k]);

@@ -21,6 +21,7 @@ int fail(int code, const char* fmt, ...);
 
 typedef void (*oms_fn)(const OmsTables, const OmsJob);
 typedef void (*sp_fn)(const SpTables, const SpJob);
+typedef void (*rt_fn)(const RtLaunch);
 
 struct OmsLaunch {
     int max_threads, min_blocks;   // __launch_bounds__ of this compilation
@@ -84,6 +85,13 @@ struct ldpc_ctx {
     int oms_threads = 0, oms_smem = 0, oms_ctas = 0;
     uint32_t beta2 = 0, maxv2 = 0;
     bool beta0 = false;
+    // int8 offset min-sum over run-time tables (shapes without a compiled kernel)
+    bool oms_rt = false;
+    ldpc::RtCode* d_rt_code = nullptr;
+    ldpc::rt_fn rt_kernel = nullptr;
+    int rt_threads = 0, rt_smem = 0, rt_ctas = 0, rt_G = 0;
+    uint32_t* d_rt_scratch = nullptr;           // check messages of large codes (global)
+    long long rt_words_per_cta = 0;
     // float decoders
     ldpc::SpTables spt;
     ldpc::sp_fn sp_kernel = nullptr;
@@ -114,6 +122,19 @@ struct ldpc_ctx {
 namespace ldpc {
 int setup_oms(ldpc_ctx* x);
 int launch_oms(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s);
+int setup_oms_rt(ldpc_ctx* x);
+int launch_oms_rt(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s);
+// Fill `out` for one code: int8 offset beta8[l] per layer (nullptr: beta8_all on every
+// layer), Max8 as half2 bits, G codeword pairs per CTA.
+int make_rt_code(const ldpc_code& c, int max_iter, uint32_t maxv2, const int* beta8, int beta8_all, int G, RtCode* out);
+// Largest row weight the run-time kernels unroll for (0: unsupported).
+int rt_dmax(int max_row_weight);
+constexpr int kRtMaxThreads = 512;          // __launch_bounds__ of oms_rt_kernel
+constexpr int kRtMaxSmem = 200 * 1024;      // dynamic shared memory the run-time kernels may use
+rt_fn rt_kernel_for(int dmax, bool quirk, bool rsmem);
+int rt_stride(int n, int G);
+// dynamic shared memory of one CTA: tables, G pairs of posteriors and staging, messages if rsmem
+size_t rt_smem_bytes(int n, int G, int E, int threads, bool rsmem);
 int setup_sp(ldpc_ctx* x);
 int launch_sp(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s);
 int setup_gen(ldpc_ctx* x);
@@ -121,4 +142,5 @@ int launch_gen(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* snr_
                int8_t* llr_i8, float* llr_f32, uint32_t* data_bits, unsigned long long* uncoded, cudaStream_t s);
 void release_gen(ldpc_ctx* x);
 uint32_t half2_bits(float v);
+int8_t max_row_i8(float max_row_metric);   // decode_row's Max_row_simd, int8 build
 }  // namespace ldpc
