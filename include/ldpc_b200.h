@@ -148,6 +148,59 @@ int ldpc_decode_f32_host(ldpc_ctx *ctx, const float *llr, size_t n, float *post_
 int ldpc_decode_set_compat(ldpc_ctx *ctx, void *decoded_metrics, unsigned num_codeword, unsigned simd_par,
                            uint64_t *tot_iter);
 
+/* ---- batched decoding of several codes in one launch ----------------------
+ *
+ * No counterpart in the reference: it runs one code per process
+ * (build/run_LDPCsim.pl:102-109) and one codeword at a time
+ * (LDPCdecode.cpp:227-243).  A batch holds several codes, each with its own
+ * configuration (int8 offset min-sum only) and optionally one int8 offset
+ * per layer (learned offsets).  A plan fixes a list of jobs (device buffers
+ * of one code each) and splits them into chunks of equal work.  A plan's
+ * launch is ONE persistent kernel over all jobs, and it can be replayed
+ * from a CUDA graph.  Per codeword, the results are exactly those of
+ * ldpc_decode_int8 / ldpc_decode_count on that code. */
+typedef struct ldpc_batch ldpc_batch;
+typedef struct ldpc_batch_plan ldpc_batch_plan;
+
+typedef struct {
+    int code;                       /* index of the code in the batch */
+    const int8_t *llr;              /* dev [n][N_code] */
+    size_t n;
+    int8_t *post_out;               /* dev, optional (NULL) */
+    uint32_t *hard_out;             /* dev [n][hard_words], optional */
+    uint8_t *iters_out;             /* dev [n], optional */
+    const uint32_t *data_bits;      /* dev, optional: fused counting as ldpc_decode_count */
+    size_t ref_period;
+    size_t bucket_size;
+    unsigned long long *counters;   /* dev [n_buckets][4], accumulated */
+    int n_buckets;
+} ldpc_batch_job;
+
+int ldpc_batch_create(const ldpc_code *const *codes, const ldpc_cfg *cfgs, int n_codes, int device,
+                      ldpc_batch **out);
+/* One int8 offset per layer of code `code` (values truncated like beta;
+ * 0..127).  NULL restores cfg.beta on every layer.  It affects plans
+ * created afterwards. */
+int ldpc_batch_set_offsets(ldpc_batch *b, int code, const float *beta_per_layer);
+void ldpc_batch_destroy(ldpc_batch *b);
+
+/* Plan over `jobs`.  threads = CTA width (0: the autotuned or default value);
+ * chunks_per_cta = work chunks per resident CTA (0: tuned or 2). */
+int ldpc_batch_plan_create(ldpc_batch *b, const ldpc_batch_job *jobs, int n_jobs, int threads, int chunks_per_cta,
+                           ldpc_batch_plan **out);
+int ldpc_batch_plan_launch(ldpc_batch_plan *p, void *stream);
+/* The first call captures the launch into a CUDA graph; every call replays
+ * it, ordered after the work already on `stream`. */
+int ldpc_batch_plan_graph_launch(ldpc_batch_plan *p, void *stream);
+void ldpc_batch_plan_destroy(ldpc_batch_plan *p);
+
+/* Project autotuner: times plans over the first `sample` codewords of each
+ * job (outputs not written) for every CTA width in {128..512} that fits and
+ * 1, 2 or 4 chunks per CTA.  It keeps the fastest setting for later plans
+ * and reports it (any output pointer may be NULL). */
+int ldpc_batch_autotune(ldpc_batch *b, const ldpc_batch_job *jobs, int n_jobs, size_t sample, int *threads,
+                        int *chunks_per_cta, double *ms);
+
 /* ---- channel generation -------------------------------------------------- */
 
 /* Fused generation: random data bits, QC encoding, BPSK, AWGN and LLR

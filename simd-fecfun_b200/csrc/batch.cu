@@ -1,0 +1,363 @@
+// Batched decoding: several codes (and Z sizes) in one persistent launch of
+// the run-time-table int8 kernel, plans with CUDA-graph replay, and the
+// launch-shape autotuner.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "internal.h"
+
+using ldpc::fail;
+
+struct ldpc_batch {
+    int device = 0, sms = 0;
+    std::vector<ldpc_code> codes;
+    std::vector<ldpc_cfg> cfgs;
+    std::vector<std::vector<int>> beta8;     // per code, per layer
+    std::vector<uint32_t> maxv2;
+    int tuned_threads = 0, tuned_cpc = 0;
+};
+
+struct ldpc_batch_plan {
+    int device = 0;
+    ldpc::RtLaunch lp;
+    ldpc::rt_fn k = nullptr;
+    int threads = 0, smem = 0, grid = 0;
+    ldpc::RtCode* d_codes = nullptr;
+    ldpc::RtJob* d_jobs = nullptr;
+    ldpc::RtChunk* d_chunks = nullptr;
+    uint32_t* d_scratch = nullptr;
+    cudaStream_t own = nullptr;              // graph capture and replay stream
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+constexpr int kTunedWidths[] = {128, 192, 256, 320, 384, 448, 512};
+
+// Chunks of about equal work (codewords x edges per codeword) so that the
+// strided chunk-to-CTA assignment balances the CTAs.
+void make_chunks(const std::vector<ldpc::RtJob>& jobs, const std::vector<long long>& cost_per_cw,
+                 const std::vector<int>& min_chunk, long long target_chunks, std::vector<ldpc::RtChunk>& out) {
+    double total = 0;
+    for (size_t j = 0; j < jobs.size(); ++j) total += (double)jobs[j].ncw * (double)cost_per_cw[j];
+    const double per_chunk = std::max(1.0, total / (double)std::max(1LL, target_chunks));
+    for (size_t j = 0; j < jobs.size(); ++j) {
+        const long long n = jobs[j].ncw;
+        if (n == 0) continue;
+        long long m = (long long)std::llround((double)n * (double)cost_per_cw[j] / per_chunk);
+        m = std::max(1LL, std::min(m, std::max(1LL, n / min_chunk[j])));
+        for (long long i = 0; i < m; ++i) {
+            ldpc::RtChunk c;
+            c.job = (int)j;
+            c.pad = 0;
+            c.lo = n * i / m;
+            c.hi = n * (i + 1) / m;
+            out.push_back(c);
+        }
+    }
+}
+
+int check_job(const ldpc_batch* b, const ldpc_batch_job& j, int idx) {
+    if (j.code < 0 || j.code >= (int)b->codes.size()) return fail(LDPC_ERR_INVALID_ARG, "job %d: code %d of %zu", idx, j.code, b->codes.size());
+    if (j.n && !j.llr) return fail(LDPC_ERR_INVALID_ARG, "job %d: llr is NULL", idx);
+    if (j.n > (size_t)1 << 40) return fail(LDPC_ERR_INVALID_ARG, "job %d: n=%zu too large", idx, j.n);
+    if (j.counters && (!j.data_bits || j.ref_period == 0 || j.n_buckets < 1 || j.n_buckets > ldpc::OMS_MAX_BUCKETS))
+        return fail(LDPC_ERR_INVALID_ARG, "job %d: counting needs data_bits, ref_period > 0 and 1..%d buckets", idx,
+                    ldpc::OMS_MAX_BUCKETS);
+    return LDPC_OK;
+}
+
+void release(ldpc_batch_plan* p) {
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    if (p->ev_in) cudaEventDestroy(p->ev_in);
+    if (p->ev_out) cudaEventDestroy(p->ev_out);
+    if (p->own) cudaStreamDestroy(p->own);
+    cudaFree(p->d_codes);
+    cudaFree(p->d_jobs);
+    cudaFree(p->d_chunks);
+    cudaFree(p->d_scratch);
+}
+
+struct PlanDel {
+    void operator()(ldpc_batch_plan* p) const {
+        if (p) {
+            cudaSetDevice(p->device);
+            release(p);
+            delete p;
+        }
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+int ldpc_batch_create(const ldpc_code* const* codes, const ldpc_cfg* cfgs, int n_codes, int device, ldpc_batch** out) {
+    if (!codes || !cfgs || !out || n_codes < 1) return fail(LDPC_ERR_INVALID_ARG, "batch: NULL argument or no codes");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(LDPC_ERR_CUDA, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev) return fail(LDPC_ERR_INVALID_ARG, "device %d of %d", device, ndev);
+    std::unique_ptr<ldpc_batch> b(new ldpc_batch);
+    b->device = device;
+    CUDA_TRY(cudaSetDevice(device));
+    CUDA_TRY(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device));
+    for (int i = 0; i < n_codes; ++i) {
+        if (!codes[i]) return fail(LDPC_ERR_INVALID_ARG, "batch: code %d is NULL", i);
+        const ldpc_code& c = *codes[i];
+        const ldpc_cfg& g = cfgs[i];
+        if (g.variant != LDPC_INT8_OMS) return fail(LDPC_ERR_UNSUPPORTED, "batch: code %d: only the int8 decoder is batched", i);
+        if (g.max_iter < 1 || g.max_iter > 255) return fail(LDPC_ERR_UNSUPPORTED, "batch: code %d: max_iter=%u", i, g.max_iter);
+        if (!(g.beta >= 0.0f && g.beta < 128.0f)) return fail(LDPC_ERR_UNSUPPORTED, "batch: code %d: beta=%g", i, g.beta);
+        if (!(g.max_row_metric > -128.0f && g.max_row_metric < 128.0f))
+            return fail(LDPC_ERR_UNSUPPORTED, "batch: code %d: max_row_metric=%g", i, g.max_row_metric);
+        const int max8 = ldpc::max_row_i8(g.max_row_metric);
+        if (max8 < 0) return fail(LDPC_ERR_UNSUPPORTED, "batch: code %d: negative row clamp", i);
+        if (!ldpc::rt_dmax(c.max_row_weight) || c.z > ldpc::RT_MAX_Z || c.mrow > ldpc::RT_MAX_L ||
+            (int)c.row_cols.size() > ldpc::RT_MAX_E)
+            return fail(LDPC_ERR_UNSUPPORTED, "batch: code %d (Z=%d, %d layers, weight %d) exceeds the kernel's tables", i,
+                        c.z, c.mrow, c.max_row_weight);
+        b->codes.push_back(c);
+        b->cfgs.push_back(g);
+        b->beta8.push_back(std::vector<int>(c.mrow, (int)(int8_t)g.beta));
+        b->maxv2.push_back(ldpc::half2_bits((float)max8));
+    }
+    *out = b.release();
+    return LDPC_OK;
+}
+
+int ldpc_batch_set_offsets(ldpc_batch* b, int code, const float* beta) {
+    if (!b) return fail(LDPC_ERR_INVALID_ARG, "batch is NULL");
+    if (code < 0 || code >= (int)b->codes.size()) return fail(LDPC_ERR_INVALID_ARG, "code %d of %zu", code, b->codes.size());
+    std::vector<int>& v = b->beta8[code];
+    for (size_t l = 0; l < v.size(); ++l) {
+        const float f = beta ? beta[l] : b->cfgs[code].beta;
+        if (!(f >= 0.0f && f < 128.0f)) return fail(LDPC_ERR_UNSUPPORTED, "offset %g of layer %zu outside [0, 128)", f, l);
+    }
+    for (size_t l = 0; l < v.size(); ++l) v[l] = (int)(int8_t)(beta ? beta[l] : b->cfgs[code].beta);
+    return LDPC_OK;
+}
+
+void ldpc_batch_destroy(ldpc_batch* b) { delete b; }
+
+int ldpc_batch_plan_create(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int threads, int cpc,
+                           ldpc_batch_plan** out) {
+    if (!b || !out || (n_jobs > 0 && !jobs) || n_jobs < 0) return fail(LDPC_ERR_INVALID_ARG, "batch plan: NULL argument");
+    *out = nullptr;
+    for (int i = 0; i < n_jobs; ++i)
+        if (int rc = check_job(b, jobs[i], i)) return rc;
+    CUDA_TRY(cudaSetDevice(b->device));
+    // codes used by the jobs
+    const int nc = (int)b->codes.size();
+    int maxz = 0;
+    for (int i = 0; i < n_jobs; ++i) maxz = std::max(maxz, b->codes[jobs[i].code].z);
+    if (threads <= 0) threads = b->tuned_threads;
+    if (threads <= 0) threads = std::max(256, ((maxz + 31) / 32) * 32);
+    if (cpc <= 0) cpc = b->tuned_cpc > 0 ? b->tuned_cpc : 2;
+    if (threads % 32 || threads > ldpc::kRtMaxThreads || threads < maxz)
+        return fail(LDPC_ERR_UNSUPPORTED, "batch plan: %d threads per CTA (multiple of 32, >= Z=%d, <= %d)", threads, maxz,
+                    ldpc::kRtMaxThreads);
+    std::vector<int> G(nc, 1);
+    int dmax = 8, maxE = 0;
+    bool quirk = false, rsmem = true;
+    for (int c = 0; c < nc; ++c) {
+        const ldpc_code& cd = b->codes[c];
+        const int n = cd.z * cd.mcol, E = (int)cd.row_cols.size();
+        G[c] = std::max(1, std::min(16, threads / cd.z));
+        while (G[c] > 1 && ldpc::rt_smem_bytes(n, G[c], E, 0, false) > (size_t)ldpc::kRtMaxSmem) --G[c];
+        if (ldpc::rt_smem_bytes(n, G[c], E, 0, false) > (size_t)ldpc::kRtMaxSmem)
+            return fail(LDPC_ERR_UNSUPPORTED, "batch plan: code %d (N=%d) does not fit shared memory", c, n);
+        if (ldpc::rt_smem_bytes(n, G[c], E, threads, true) > (size_t)ldpc::kRtMaxSmem) rsmem = false;
+        dmax = std::max(dmax, ldpc::rt_dmax(cd.max_row_weight));
+        maxE = std::max(maxE, E);
+        for (int v : b->beta8[c]) quirk |= v == 0;
+    }
+    size_t smem = 0;
+    for (int c = 0; c < nc; ++c) {
+        const ldpc_code& cd = b->codes[c];
+        smem = std::max(smem, ldpc::rt_smem_bytes(cd.z * cd.mcol, G[c], (int)cd.row_cols.size(), threads, rsmem));
+    }
+    std::unique_ptr<ldpc_batch_plan, PlanDel> p(new ldpc_batch_plan);
+    p->device = b->device;
+    p->k = ldpc::rt_kernel_for(dmax, quirk, rsmem);
+    p->threads = threads;
+    p->smem = (int)smem;
+    CUDA_TRY(cudaFuncSetAttribute((const void*)p->k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)p->k, threads, smem));
+    if (per_sm < 1) return fail(LDPC_ERR_UNSUPPORTED, "batch plan: %d threads x %zu B do not fit an SM", threads, smem);
+    const long long ctas = (long long)per_sm * b->sms;
+
+    std::vector<ldpc::RtCode> hc(nc);
+    for (int c = 0; c < nc; ++c) {
+        const ldpc_code& cd = b->codes[c];
+        if (int rc = ldpc::make_rt_code(cd, (int)b->cfgs[c].max_iter, b->maxv2[c], b->beta8[c].data(), 0, G[c], &hc[c]))
+            return rc;
+    }
+    std::vector<ldpc::RtJob> hj(n_jobs);
+    std::vector<long long> cost(n_jobs);
+    std::vector<int> minc(n_jobs);
+    for (int i = 0; i < n_jobs; ++i) {
+        const ldpc_batch_job& s = jobs[i];
+        ldpc::RtJob& j = hj[i];
+        memset(&j, 0, sizeof(j));
+        j.llr = s.llr;
+        j.ncw = (long long)s.n;
+        j.post_out = s.post_out;
+        j.hard_out = s.hard_out;
+        j.iters_out = s.iters_out;
+        j.ref_bits = s.data_bits;
+        j.ref_period = s.ref_period > 0 ? (long long)s.ref_period : 1;
+        j.bucket_size = s.bucket_size > 0 ? (long long)s.bucket_size : std::max(1LL, (long long)s.n);
+        j.counters = s.counters;
+        j.n_buckets = std::max(1, std::min(s.n_buckets, ldpc::OMS_MAX_BUCKETS));
+        j.code = s.code;
+        const ldpc_code& cd = b->codes[s.code];
+        cost[i] = (long long)cd.row_cols.size() * cd.z;
+        minc[i] = 8 * G[s.code];     // a chunk keeps its 2G slots busy for a while
+    }
+    std::vector<ldpc::RtChunk> chunks;
+    make_chunks(hj, cost, minc, ctas * cpc, chunks);
+    const int n_chunks = (int)chunks.size();
+    p->grid = (int)std::max(1LL, std::min<long long>(ctas, n_chunks));
+    CUDA_TRY(cudaMalloc(&p->d_codes, sizeof(ldpc::RtCode) * nc));
+    CUDA_TRY(cudaMemcpy(p->d_codes, hc.data(), sizeof(ldpc::RtCode) * nc, cudaMemcpyHostToDevice));
+    if (n_jobs) {
+        CUDA_TRY(cudaMalloc(&p->d_jobs, sizeof(ldpc::RtJob) * n_jobs));
+        CUDA_TRY(cudaMemcpy(p->d_jobs, hj.data(), sizeof(ldpc::RtJob) * n_jobs, cudaMemcpyHostToDevice));
+    }
+    if (n_chunks) {
+        CUDA_TRY(cudaMalloc(&p->d_chunks, sizeof(ldpc::RtChunk) * n_chunks));
+        CUDA_TRY(cudaMemcpy(p->d_chunks, chunks.data(), sizeof(ldpc::RtChunk) * n_chunks, cudaMemcpyHostToDevice));
+    }
+    long long words = 0;
+    if (!rsmem) {
+        words = (long long)maxE * threads;
+        CUDA_TRY(cudaMalloc(&p->d_scratch, (size_t)p->grid * words * 4));
+    }
+    memset(&p->lp, 0, sizeof(p->lp));
+    p->lp.codes = p->d_codes;
+    p->lp.jobs = p->d_jobs;
+    p->lp.chunks = p->d_chunks;
+    p->lp.n_chunks = n_chunks;
+    p->lp.r_scratch = p->d_scratch;
+    p->lp.r_words_per_cta = words;
+    if (!p->d_jobs) p->lp.n_chunks = 0;
+    *out = p.release();
+    return LDPC_OK;
+}
+
+int ldpc_batch_plan_launch(ldpc_batch_plan* p, void* stream) {
+    if (!p) return fail(LDPC_ERR_INVALID_ARG, "plan is NULL");
+    if (!p->lp.jobs || p->lp.n_chunks == 0) return LDPC_OK;
+    CUDA_TRY(cudaSetDevice(p->device));
+    p->k<<<p->grid, p->threads, p->smem, (cudaStream_t)stream>>>(p->lp);
+    CUDA_TRY(cudaGetLastError());
+    return LDPC_OK;
+}
+
+int ldpc_batch_plan_graph_launch(ldpc_batch_plan* p, void* stream) {
+    if (!p) return fail(LDPC_ERR_INVALID_ARG, "plan is NULL");
+    if (!p->lp.jobs || p->lp.n_chunks == 0) return LDPC_OK;
+    CUDA_TRY(cudaSetDevice(p->device));
+    if (!p->exec) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&p->own, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming));
+        CUDA_TRY(cudaStreamBeginCapture(p->own, cudaStreamCaptureModeThreadLocal));
+        p->k<<<p->grid, p->threads, p->smem, p->own>>>(p->lp);
+        const cudaError_t le = cudaGetLastError();
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(p->own, &g);
+        if (le != cudaSuccess || ce != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return fail(LDPC_ERR_CUDA, "graph capture: %s", cudaGetErrorString(le != cudaSuccess ? le : ce));
+        }
+        p->graph = g;
+        CUDA_TRY(cudaGraphInstantiate(&p->exec, p->graph, 0));
+    }
+    // replay on the plan's stream, ordered after and before the caller's stream
+    CUDA_TRY(cudaEventRecord(p->ev_in, (cudaStream_t)stream));
+    CUDA_TRY(cudaStreamWaitEvent(p->own, p->ev_in, 0));
+    CUDA_TRY(cudaGraphLaunch(p->exec, p->own));
+    CUDA_TRY(cudaEventRecord(p->ev_out, p->own));
+    CUDA_TRY(cudaStreamWaitEvent((cudaStream_t)stream, p->ev_out, 0));
+    return LDPC_OK;
+}
+
+void ldpc_batch_plan_destroy(ldpc_batch_plan* p) { PlanDel()(p); }
+
+int ldpc_batch_autotune(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, size_t sample, int* threads_out,
+                        int* cpc_out, double* ms_out) {
+    if (!b || (n_jobs > 0 && !jobs) || n_jobs < 1) return fail(LDPC_ERR_INVALID_ARG, "autotune: no jobs");
+    for (int i = 0; i < n_jobs; ++i)
+        if (int rc = check_job(b, jobs[i], i)) return rc;
+    if (sample == 0) sample = 8192;
+    std::vector<ldpc_batch_job> sj(jobs, jobs + n_jobs);
+    int maxz = 0;
+    for (ldpc_batch_job& j : sj) {
+        j.n = std::min(j.n, sample);
+        j.post_out = nullptr;
+        j.hard_out = nullptr;
+        j.iters_out = nullptr;
+        j.data_bits = nullptr;
+        j.counters = nullptr;
+        maxz = std::max(maxz, b->codes[j.code].z);
+    }
+    CUDA_TRY(cudaSetDevice(b->device));
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    double best = 1e30;
+    int best_t = 0, best_c = 0, rc = LDPC_OK;
+    const int cpcs[] = {1, 2, 4};
+    for (int t : kTunedWidths) {
+        if (t < maxz) continue;
+        for (int c : cpcs) {
+            ldpc_batch_plan* p = nullptr;
+            if (ldpc_batch_plan_create(b, sj.data(), n_jobs, t, c, &p) != LDPC_OK) continue;   // shape does not fit
+            float ms[3] = {0, 0, 0};
+            rc = ldpc_batch_plan_launch(p, s);    // warm-up
+            for (int r = 0; r < 3 && rc == LDPC_OK; ++r) {
+                cudaEventRecord(e0, s);
+                rc = ldpc_batch_plan_launch(p, s);
+                cudaEventRecord(e1, s);
+                if (cudaEventSynchronize(e1) != cudaSuccess) rc = fail(LDPC_ERR_CUDA, "autotune: launch failed");
+                else cudaEventElapsedTime(&ms[r], e0, e1);
+            }
+            ldpc_batch_plan_destroy(p);
+            if (rc != LDPC_OK) break;
+            std::sort(ms, ms + 3);
+            if (ms[1] < best) {
+                best = ms[1];
+                best_t = t;
+                best_c = c;
+            }
+        }
+        if (rc != LDPC_OK) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    if (rc != LDPC_OK) return rc;
+    if (!best_t) return fail(LDPC_ERR_UNSUPPORTED, "autotune: no launch shape fits these codes");
+    b->tuned_threads = best_t;
+    b->tuned_cpc = best_c;
+    if (threads_out) *threads_out = best_t;
+    if (cpc_out) *cpc_out = best_c;
+    if (ms_out) *ms_out = best;
+    return LDPC_OK;
+}
+
+}  // extern "C"

@@ -9,7 +9,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
-from typing import Optional
+from typing import Optional, Sequence
 
 import numpy as np
 
@@ -56,6 +56,13 @@ class SnrStats(C.Structure):
 
 _vp = C.c_void_p
 _sz = C.c_size_t
+
+
+class BatchJob(C.Structure):
+    _fields_ = [("code", C.c_int), ("llr", _vp), ("n", _sz), ("post_out", _vp), ("hard_out", _vp), ("iters_out", _vp),
+                ("data_bits", _vp), ("ref_period", _sz), ("bucket_size", _sz), ("counters", _vp), ("n_buckets", C.c_int)]
+
+
 _PROTOS = {
     "ldpc_last_error": (C.c_char_p, []),
     "ldpc_device_count": (C.c_int, [C.POINTER(C.c_int)]),
@@ -78,6 +85,15 @@ _PROTOS = {
     "ldpc_decode_count": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _sz, _sz, _vp, C.c_int, _vp]),
     "ldpc_probe_int32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     "ldpc_decode_f32_noalloc": (C.c_int, [_vp, C.POINTER(Cfg), _vp, _sz, _vp, _vp, _vp, _vp]),
+    "ldpc_batch_create": (C.c_int, [C.POINTER(_vp), C.POINTER(Cfg), C.c_int, C.c_int, C.POINTER(_vp)]),
+    "ldpc_batch_set_offsets": (C.c_int, [_vp, C.c_int, _vp]),
+    "ldpc_batch_destroy": (None, [_vp]),
+    "ldpc_batch_plan_create": (C.c_int, [_vp, C.POINTER(BatchJob), C.c_int, C.c_int, C.c_int, C.POINTER(_vp)]),
+    "ldpc_batch_plan_launch": (C.c_int, [_vp, _vp]),
+    "ldpc_batch_plan_graph_launch": (C.c_int, [_vp, _vp]),
+    "ldpc_batch_plan_destroy": (None, [_vp]),
+    "ldpc_batch_autotune": (C.c_int, [_vp, C.POINTER(BatchJob), C.c_int, _sz, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_double)]),
 }
 
 if not os.path.exists(LIB_PATH):
@@ -244,3 +260,86 @@ class Context:
         tot = C.c_uint64()
         check(lib.ldpc_decode_set_compat(self.h, metrics.ctypes.data, num_codeword, simd_par, C.byref(tot)))
         return tot.value
+
+
+class Batch:
+    """Several codes decoded by one persistent launch (ldpc_batch_*, int8
+    offset min-sum).  ``cfgs`` holds one dict of Context keyword arguments
+    (max_iter, max_row_metric, beta) per code."""
+
+    def __init__(self, codes: Sequence["Code"], cfgs: Sequence[dict], device: int = 0):
+        if len(codes) != len(cfgs):
+            raise ValueError("one configuration per code")
+        self.codes = list(codes)
+        arr = (_vp * len(codes))(*[c.h for c in codes])
+        cf = (Cfg * len(codes))()
+        for i, k in enumerate(cfgs):
+            cf[i] = Cfg(LDPC_INT8_OMS, k.get("max_iter", 10), k.get("max_row_metric", 31.0), k.get("beta", 1.0),
+                        k.get("llr_scale", 2.0), k.get("max_abs_llr", 24.0))
+        h = _vp()
+        check(lib.ldpc_batch_create(arr, cf, len(codes), device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.ldpc_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_offsets(self, code: int, beta_per_layer=None):
+        if beta_per_layer is None:
+            check(lib.ldpc_batch_set_offsets(self.h, code, None))
+            return
+        b = np.ascontiguousarray(beta_per_layer, dtype=np.float32)
+        check(lib.ldpc_batch_set_offsets(self.h, code, b.ctypes.data))
+
+    @staticmethod
+    def _jobs(specs):
+        arr = (BatchJob * max(1, len(specs)))()
+        for i, s in enumerate(specs):
+            arr[i] = BatchJob(s["code"], _ptr(s["llr"]), s["n"], _ptr(s.get("post")), _ptr(s.get("hard")),
+                              _ptr(s.get("iters")), _ptr(s.get("data_bits")), s.get("ref_period", 0),
+                              s.get("bucket_size", 0), _ptr(s.get("counters")), s.get("n_buckets", 1))
+        return arr
+
+    def plan(self, specs, threads: int = 0, chunks_per_cta: int = 0) -> "BatchPlan":
+        """specs: dicts with code, llr, n and optional post/hard/iters/data_bits/
+        ref_period/bucket_size/counters/n_buckets (torch tensors or pointers)."""
+        arr = self._jobs(specs)
+        h = _vp()
+        check(lib.ldpc_batch_plan_create(self.h, arr, len(specs), threads, chunks_per_cta, C.byref(h)))
+        return BatchPlan(h, self)
+
+    def autotune(self, specs, sample: int = 8192):
+        arr = self._jobs(specs)
+        t, c, ms = C.c_int(), C.c_int(), C.c_double()
+        check(lib.ldpc_batch_autotune(self.h, arr, len(specs), sample, C.byref(t), C.byref(c), C.byref(ms)))
+        return t.value, c.value, ms.value
+
+
+class BatchPlan:
+    def __init__(self, h, batch: Batch):
+        self.h = h
+        self.batch = batch
+
+    def launch(self, stream=0):
+        check(lib.ldpc_batch_plan_launch(self.h, stream or None))
+
+    def graph_launch(self, stream=0):
+        check(lib.ldpc_batch_plan_graph_launch(self.h, stream or None))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.ldpc_batch_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
