@@ -201,6 +201,40 @@ void ldpc_batch_plan_destroy(ldpc_batch_plan *p);
 int ldpc_batch_autotune(ldpc_batch *b, const ldpc_batch_job *jobs, int n_jobs, size_t sample, int *threads,
                         int *chunks_per_cta, double *ms);
 
+/* ---- learned offsets: differentiable unrolled float offset min-sum --------
+ *
+ * No counterpart in the reference, whose decode_row has one offset for every
+ * layer and iteration (decode_functions.cpp:59-62).  The context must use
+ * LDPC_F32_OMS; its max_row_metric is the row clamp.  beta is a device array
+ * [iters][mrow] of offsets.  The decoder runs exactly `iters` iterations
+ * (no early exit), so the loss is a fixed function of beta.
+ *
+ * ldpc_learned_forward writes per-iteration checkpoints:
+ *   ckpt_p [iters+1][n][N]   posteriors at the start of each iteration,
+ *                            plus the final ones;
+ *   ckpt_r [iters][n][E]     check messages at the start of each iteration
+ *                            (E = ldpc_code_info.edges).
+ *
+ * ldpc_learned_backward returns the gradient of
+ *   L = sum_it loss_w[it] * inv_norm * sum_cw sum_v softplus(-(1 - 2 c_v) P_it+1[v])
+ * (binary cross-entropy of the posteriors after every iteration; c = sent
+ * code bits, cw_bits [n][N] 0/1).  For each iteration it recomputes the
+ * layers from its checkpoint, then runs the adjoint in reverse.
+ * gbeta_part [grid][iters*mrow] receives one partial sum per CTA (grid from
+ * ldpc_learned_grid); their column sums are dL/dbeta, reduced in a fixed
+ * order, so results are deterministic.  grad_llr [n][N] (optional) receives
+ * dL/dLLR. */
+int ldpc_learned_grid(ldpc_ctx *ctx, size_t n, int *bwd_grid);
+int ldpc_learned_forward(ldpc_ctx *ctx, const float *llr, size_t n, int iters, const float *beta, float *ckpt_p,
+                         float *ckpt_r, void *stream);
+int ldpc_learned_backward(ldpc_ctx *ctx, size_t n, int iters, const float *beta, const float *ckpt_p,
+                          const float *ckpt_r, const uint8_t *cw_bits, const float *loss_w, float inv_norm,
+                          float *gbeta_part, float *grad_llr, void *stream);
+/* Decoding with learned offsets: up to `iters` iterations with early exit on
+ * the syndrome, as the float decoders do; outputs as ldpc_decode_f32. */
+int ldpc_learned_decode(ldpc_ctx *ctx, const float *llr, size_t n, int iters, const float *beta, float *post_out,
+                        uint32_t *hard_out, uint8_t *iters_out, void *stream);
+
 /* ---- channel generation -------------------------------------------------- */
 
 /* Fused generation: random data bits, QC encoding, BPSK, AWGN and LLR

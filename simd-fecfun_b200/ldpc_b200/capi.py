@@ -92,6 +92,10 @@ _PROTOS = {
     "ldpc_batch_plan_launch": (C.c_int, [_vp, _vp]),
     "ldpc_batch_plan_graph_launch": (C.c_int, [_vp, _vp]),
     "ldpc_batch_plan_destroy": (None, [_vp]),
+    "ldpc_learned_grid": (C.c_int, [_vp, _sz, C.POINTER(C.c_int)]),
+    "ldpc_learned_forward": (C.c_int, [_vp, _vp, _sz, C.c_int, _vp, _vp, _vp, _vp]),
+    "ldpc_learned_backward": (C.c_int, [_vp, _sz, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_float, _vp, _vp, _vp]),
+    "ldpc_learned_decode": (C.c_int, [_vp, _vp, _sz, C.c_int, _vp, _vp, _vp, _vp, _vp]),
     "ldpc_batch_autotune": (C.c_int, [_vp, C.POINTER(BatchJob), C.c_int, _sz, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                       C.POINTER(C.c_double)]),
 }
