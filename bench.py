@@ -218,6 +218,27 @@ def run_reference(args):
     return 0
 
 
+def run_workload(args):
+    """The other measured workloads (ldpc_b200.workloads), on one GPU; under
+    torchrun only rank 0 runs."""
+    ws, rank, local = _dist()
+    if rank != 0:
+        return 0
+    import torch
+    from ldpc_b200 import workloads
+    torch.cuda.set_device(local)
+    clk = _clock_sampler(local)
+    if args.workload == "nr-mix":
+        out = workloads.nr_mix(steps=args.steps, warmup=args.warmup)
+    elif args.workload == "hetero-mix":
+        out = workloads.hetero_mix(steps=args.steps, warmup=args.warmup)
+    else:
+        out = workloads.learned_run(train_steps=max(args.steps, 5))
+    out["clocks"] = _clock_summary(clk)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -230,9 +251,14 @@ def main():
     ap.add_argument("--cpu-reps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="11ad", choices=["11ad", "nr-mix", "hetero-mix", "learned"],
+                    help="11ad: the headline run; others: the batched 5G NR mix, the 18-code 802.11 mix "
+                         "(plain vs learned offsets), learned-offset training (one GPU)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "11ad":
+        return run_workload(args)
 
     import numpy as np
     import torch

@@ -191,7 +191,7 @@ int ldpc_batch_plan_create(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs
     p->k = ldpc::rt_kernel_for(dmax, quirk, rsmem);
     p->threads = threads;
     p->smem = (int)smem;
-    CUDA_TRY(cudaFuncSetAttribute((const void*)p->k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_TRY(ldpc::allow_dynamic_smem((const void*)p->k, ldpc::kRtMaxSmem));
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)p->k, threads, smem));
     if (per_sm < 1) return fail(LDPC_ERR_UNSUPPORTED, "batch plan: %d threads x %zu B do not fit an SM", threads, smem);

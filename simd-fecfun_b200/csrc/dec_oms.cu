@@ -145,7 +145,8 @@ int setup_oms(ldpc_ctx* x) {
     x->oms_threads = ((G * c.z + 31) / 32) * 32;
     // posteriors + LLR staging + shared-memory check messages
     x->oms_smem = ((G * stride * 4 + 15) & ~15) + 2 * G * ((t.n + 15) & ~15) + best->smem_edges * x->oms_threads * 4;
-    CUDA_TRY(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, x->oms_smem));
+    if (x->oms_smem > kOmsMaxSmem) return fail(LDPC_ERR_UNSUPPORTED, "int8 decoder: %d B of shared memory", x->oms_smem);
+    CUDA_TRY(allow_dynamic_smem((const void*)k, kOmsMaxSmem));
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k, x->oms_threads, x->oms_smem));
     if (per_sm < 1)

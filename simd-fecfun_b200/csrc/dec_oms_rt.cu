@@ -99,7 +99,7 @@ int setup_oms_rt(ldpc_ctx* x) {
     int rc = make_rt_code(c, (int)x->cfg.max_iter, x->maxv2, nullptr, (int)(int8_t)x->cfg.beta, G, &host);
     if (rc) return rc;
     rt_fn k = rt_kernel_for(dmax, x->beta0, rsmem);
-    CUDA_TRY(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_TRY(allow_dynamic_smem((const void*)k, kRtMaxSmem));
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k, threads, smem));
     if (per_sm < 1) return fail(LDPC_ERR_UNSUPPORTED, "int8 decoder: %d threads x %zu B do not fit an SM", threads, smem);

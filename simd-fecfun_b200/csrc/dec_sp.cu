@@ -67,8 +67,8 @@ int setup_sp(ldpc_ctx* x) {
     x->sp_kernel = v->k;
     x->sp_smem = (int)(base_smem + (rsmem ? r_smem : 0));
     // up to 220 KB dynamic (B200: 227 KB per CTA, less the kernel's static shared memory)
-    if (x->sp_smem > 220 * 1024) return fail(LDPC_ERR_UNSUPPORTED, "float decoder: %d B of shared memory", x->sp_smem);
-    CUDA_TRY(cudaFuncSetAttribute((const void*)v->k, cudaFuncAttributeMaxDynamicSharedMemorySize, x->sp_smem));
+    if (x->sp_smem > kSpMaxSmem) return fail(LDPC_ERR_UNSUPPORTED, "float decoder: %d B of shared memory", x->sp_smem);
+    CUDA_TRY(allow_dynamic_smem((const void*)v->k, kSpMaxSmem));
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)v->k, x->sp_threads, x->sp_smem));
     if (per_sm < 1) return fail(LDPC_ERR_UNSUPPORTED, "float decoder: launch does not fit an SM");

@@ -62,8 +62,8 @@ int setup_gen(ldpc_ctx* x) {
     int smem = 0;
     gen_grid(x, 1, &smem);
     if (smem > 200 * 1024) return fail(LDPC_ERR_UNSUPPORTED, "generator needs %d B of shared memory", smem);
-    CUDA_TRY(cudaFuncSetAttribute((const void*)gen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CUDA_TRY(cudaFuncSetAttribute((const void*)encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(allow_dynamic_smem((const void*)gen_kernel, 200 * 1024));
+    CUDA_TRY(allow_dynamic_smem((const void*)encode_kernel, 200 * 1024));
     return LDPC_OK;
 }
 

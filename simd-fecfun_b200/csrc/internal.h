@@ -23,6 +23,16 @@ typedef void (*oms_fn)(const OmsTables, const OmsJob);
 typedef void (*sp_fn)(const SpTables, const SpJob);
 typedef void (*rt_fn)(const RtLaunch);
 
+// The dynamic shared-memory limit is an attribute of the kernel function,
+// shared by every context that launches it: set it to the most any launch of
+// that kernel may use (never to one context's size, which a later context
+// with a smaller size would lower under the first one's launches).
+inline cudaError_t allow_dynamic_smem(const void* fn, int bytes) {
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+constexpr int kOmsMaxSmem = 200 * 1024;     // int8 register-shape kernels
+constexpr int kSpMaxSmem = 220 * 1024;      // float decoders (B200: 227 KB per CTA less static shared memory)
+
 struct OmsLaunch {
     int max_threads, min_blocks;   // __launch_bounds__ of this compilation
     oms_fn k_beta, k_beta0;

@@ -13,6 +13,8 @@
 //     b, b + grid, ...; within a chunk the persistent slot refill of
 //     oms_f16_kernel keeps every slot busy.
 #pragma once
+#include <type_traits>
+
 #include "oms_f16.cuh"
 
 namespace ldpc {
@@ -61,6 +63,37 @@ __device__ __forceinline__ void rt_layer(const RtCode& C, int l, uint32_t* Ps, u
     }
 }
 
+// Calls f(std::integral_constant<int, D>) with the smallest unrolled width D
+// >= d among 4, 6, 8, 10, 12, 16, 20, 24 and DMAX: a layer of weight d runs
+// d edge slots' worth of predicated instructions rounded up a little, not
+// DMAX (d is the same for every thread of the CTA, so the branch is uniform).
+template <int DMAX, class F>
+__device__ __forceinline__ void rt_dispatch(int d, F&& f) {
+#define RT_BUCKET(W)                                               \
+    if constexpr (DMAX > W) {                                      \
+        if (d <= W) {                                              \
+            f(std::integral_constant<int, W>{});                   \
+            return;                                                \
+        }                                                          \
+    }
+    RT_BUCKET(4) RT_BUCKET(6) RT_BUCKET(8) RT_BUCKET(10) RT_BUCKET(12) RT_BUCKET(16) RT_BUCKET(20) RT_BUCKET(24)
+#undef RT_BUCKET
+    f(std::integral_constant<int, DMAX>{});
+}
+
+template <int D>
+__device__ __forceinline__ uint32_t rt_row_parity(const RtCode& C, int d, int eb, const uint32_t* Ps, int t, int gbase, int z) {
+    uint32_t x = 0;
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+        if (j < d) {
+            const uint32_t ed = C.edge[eb + j];
+            x ^= Ps[gbase + (int)(ed >> 9) + wrap_add(t, (int)(ed & 511u), z)];
+        }
+    }
+    return x;
+}
+
 // syndrome of this thread's check rows with early exit (as oms_syndrome)
 template <int DMAX>
 __device__ __forceinline__ void rt_syndrome(const RtCode& C, const uint32_t* Ps, int t, int gbase, int z, uint32_t* synd) {
@@ -68,13 +101,7 @@ __device__ __forceinline__ void rt_syndrome(const RtCode& C, const uint32_t* Ps,
     for (int l = 0; l < C.L; ++l) {
         const int d = C.rw[l], eb = C.ebase[l];
         uint32_t x = 0;
-#pragma unroll
-        for (int j = 0; j < DMAX; ++j) {
-            if (j < d) {
-                const uint32_t ed = C.edge[eb + j];
-                x ^= Ps[gbase + (int)(ed >> 9) + wrap_add(t, (int)(ed & 511u), z)];
-            }
-        }
+        rt_dispatch<DMAX>(d, [&](auto D) { x = rt_row_parity<decltype(D)::value>(C, d, eb, Ps, t, gbase, z); });
         x &= 0x80008000u;
         if (x & ~seen) {
             atomicOr(synd, x);
@@ -171,7 +198,8 @@ __global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtL
         for (int par = 0;; par ^= 1) {
             // ---------------- one layered iteration ----------------
             for (int l = 0; l < C.L; ++l) {
-                if (active) rt_layer<DMAX, QUIRK>(C, l, Ps, Rt, nthr, t, gbase, z);
+                if (active)
+                    rt_dispatch<DMAX>(C.rw[l], [&](auto D) { rt_layer<decltype(D)::value, QUIRK>(C, l, Ps, Rt, nthr, t, gbase, z); });
                 __syncthreads();
             }
             if (tid < 16) {

@@ -48,7 +48,7 @@ int geometry(ldpc_ctx* x, size_t n, bool backward, Geometry* g) {
     g->k = backward ? tk->bwd : tk->fwd;
     g->threads = ((t.z + 31) / 32) * 32;
     g->smem = (int)smem;
-    CUDA_TRY(cudaFuncSetAttribute((const void*)g->k, cudaFuncAttributeMaxDynamicSharedMemorySize, g->smem));
+    CUDA_TRY(ldpc::allow_dynamic_smem((const void*)g->k, kTrainMaxSmem));
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)g->k, g->threads, g->smem));
     if (per_sm < 1) return fail(LDPC_ERR_UNSUPPORTED, "learned decoder: launch does not fit an SM");
