@@ -21,6 +21,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(CSRC, "_build")
 INC = os.path.join(os.path.dirname(HERE), "include")
 LIB = os.path.join(HERE, "ldpc_b200", "libldpc_b200.so")
+SIM = os.path.join(HERE, "ldpc_b200", "ldpc_sim")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
@@ -61,6 +62,14 @@ def build(force: bool = False, jobs: int = 8, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (r.stdout, r.stderr))
+    # the process-level drop-in (ldpc_sim), linked against the library next to it
+    src = os.path.join(HERE, "sim", "ldpc_sim.cpp")
+    if force or not os.path.exists(SIM) or os.path.getmtime(SIM) < max(os.path.getmtime(src), os.path.getmtime(LIB)):
+        cmd = ["g++", "-O2", "-std=c++17", "-I" + INC, src, "-o", SIM, "-L" + os.path.dirname(LIB), "-lldpc_b200",
+               "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("ldpc_sim build failed:\n%s\n%s" % (r.stdout, r.stderr))
     return LIB
 
 

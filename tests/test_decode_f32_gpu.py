@@ -80,3 +80,28 @@ def test_float_decode_count_and_generate(capi, oracle):
     cwe, be = oracle.count_errors(code, post_o, cw)
     c = cnt.cpu().numpy()[0]
     assert c[0] == n and c[1] == int(it_o.sum()) and c[2] == be and c[3] == cwe
+
+
+def test_contexts_sharing_a_kernel_keep_their_shared_memory(capi, oracle):
+    """Two live contexts whose codes run the same kernel with different
+    shared-memory sizes: creating the smaller one must not break launches of
+    the larger one (the limit belongs to the kernel, not to a context)."""
+    from ldpc_b200 import codes
+    big = codes.make_code("16e 1/2")
+    small = codes.make_code("16e 1/2", z_over=24)
+    kw = dict(variant=capi.LDPC_F32_SP, max_iter=10, max_row_metric=6e-8, beta=0.0, llr_scale=1.0, max_abs_llr=1e9)
+    ctx_big = capi.Context(capi.Code.from_tables(big), **kw)
+    ctx_small = capi.Context(capi.Code.from_tables(small), **kw)
+    for code, ctx in ((big, ctx_big), (small, ctx_small), (big, ctx_big)):
+        llr = _float_llr(code, 40, 1.25, 4, oracle)
+        post, hard, iters, tot = ctx.decode_host(llr)
+        post_o, it_o = oracle.decode_f32(code, llr, 1, 10, 6e-8, 0.0)
+        assert np.array_equal(post.view(np.uint32), post_o.view(np.uint32))
+    i8 = [codes.code_by_name("5GNR_n3136_k576"), codes.code_by_name("5GNR_n1000_k500")]
+    ctxs = [capi.Context(capi.Code.from_tables(c), max_iter=10) for c in i8]
+    from conftest import make_llr_int8
+    for c, ctx in zip(i8 + i8[:1], ctxs + ctxs[:1]):
+        llr, _, _ = make_llr_int8(c, 30, -3.0, seed=2, oracle=oracle)
+        post, hard, iters, tot = ctx.decode_host(llr)
+        post_o, it_o = oracle.decode_int8(c, llr, 10, 31.0, 1.0)
+        assert np.array_equal(post, post_o)

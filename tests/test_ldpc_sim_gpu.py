@@ -1,0 +1,47 @@
+"""ldpc_sim on the GPU: the lines it prints for the reference's stdin blob
+carry exactly the counters of ldpc_simulate with the same generator key and
+codeword offsets (one outer loop = loop_count * num_codeword codewords per
+SNR point), for the int8 and the float sum-product variants."""
+import os
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+from simblob import blob, fold_seeds, parse
+
+pytestmark = pytest.mark.gpu
+SIM = os.path.join(ROOT, "simd-fecfun_b200", "ldpc_b200", "ldpc_sim")
+
+
+@pytest.mark.parametrize("exe,name,params", [
+    ("LDPCtop_Vec64c_min_b200", "11ad 1/2", dict(mrm=31.0, scale=2.0, max_abs=24.0, beta=1.0, snr=(-1.0, 0.0, 0.5))),
+    ("LDPCtop_Vec16f_prod_b200", "16e 1/2", dict(mrm=6e-8, scale=1.0, max_abs=1e9, beta=0.0, snr=(0.5, 1.5, 0.5))),
+])
+def test_lines_match_simulate(capi, tmp_path, exe, name, params):
+    from ldpc_b200 import codes
+    code = codes.make_code(name)
+    code.write_dat(str(tmp_path / "e.dat"), str(tmp_path / "d.dat"))
+    seeds = [(0x1234567 * (i + 1)) & ((1 << 56) - 1) for i in range(64)]
+    outer, inner, ncw = 2, 3, 4000
+    s0, s1, st = params["snr"]
+    data = blob(outer, inner, ncw, 10, params["mrm"], params["scale"], params["max_abs"], params["beta"], s0, s1, st,
+                seeds, "e.dat", "d.dat")
+    os.symlink(SIM, tmp_path / exe)
+    r = subprocess.run([str(tmp_path / exe)], input=data, capture_output=True, timeout=300, cwd=tmp_path)
+    assert r.returncode == 0, r.stdout.decode()[-2000:]
+    out = parse(r.stdout.decode())
+    assert out["cw_count"] == inner * ncw and out["matrix"][:3] == (code.z, code.mcol, code.mrow)
+    snrs = [s0 + k * st for k in range(int((s1 - s0 + 1e-6) / st) + 1)]
+    assert len(out["loops"]) == outer * len(snrs)
+    variant = capi.LDPC_INT8_OMS if "64c" in exe else capi.LDPC_F32_SP
+    ctx = capi.Context(capi.Code.from_tables(code), variant=variant, max_iter=10, max_row_metric=params["mrm"],
+                       beta=params["beta"], llr_scale=params["scale"], max_abs_llr=params["max_abs"])
+    key = fold_seeds(seeds)
+    for o in range(outer):
+        ref = ctx.simulate(seed=key, cw_offset=o * inner * ncw, snr_db=snrs, n_per_snr=inner * ncw)
+        for k, st_ in enumerate(ref):
+            snr, inp, it, be, cwe, ticks = out["loops"][o * len(snrs) + k]
+            assert abs(snr - snrs[k]) < 1e-5
+            assert (inp, it, be, cwe) == (st_["uncoded_errors"], st_["iterations"], st_["bit_errors"], st_["cw_errors"])
+            assert ticks > 0
