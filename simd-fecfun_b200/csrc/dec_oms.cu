@@ -91,6 +91,7 @@ int setup_oms(ldpc_ctx* x) {
     // shapes without a register-resident instantiation: run-time tables
     if (!best || L > OMS_MAX_L || L * best->D > OMS_MAX_SLOTS_E || c.z > 640) return setup_oms_rt(x);
     x->inst = best;
+    x->oms_synd_loop = getenv("LDPC_OMS_SYND_LOOP") ? 1 : 0;
     OmsTables& t = x->omst;
     memset(&t, 0, sizeof(t));
     t.z = c.z;
@@ -179,6 +180,7 @@ int launch_oms(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s) {
     job.maxv2 = x->maxv2;
     job.queue = x->d_queue + a.queue;
     job.status = x->d_status;
+    job.synd_loop = x->oms_synd_loop;
     const long long slots = 2LL * x->omst.G;
     const long long want = ((long long)a.n + slots - 1) / slots;
     const int grid = (int)std::min<long long>(want, x->oms_ctas);

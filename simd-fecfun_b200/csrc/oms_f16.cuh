@@ -57,6 +57,10 @@ __device__ __forceinline__ uint32_t heq2_mask(uint32_t a, uint32_t b) { uint32_t
 // 1.0 in each lane where a == b, else 0.0
 __device__ __forceinline__ uint32_t heq2(uint32_t a, uint32_t b) { uint32_t d; asm("set.eq.f16x2.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); return d; }
 __device__ __forceinline__ uint32_t habs2(uint32_t a) { return a & 0x7fff7fffu; }
+// min / max of the magnitudes, with the XOR of the two sign bits as sign:
+// one instruction for |.|, the running minimum and the running sign product
+__device__ __forceinline__ uint32_t hmin2_xs(uint32_t a, uint32_t b) { uint32_t d; asm("min.xorsign.abs.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); return d; }
+__device__ __forceinline__ uint32_t hmax2_xs(uint32_t a, uint32_t b) { uint32_t d; asm("max.xorsign.abs.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); return d; }
 
 constexpr uint32_t H2_M128 = 0xd800d800u;   // -128.0 in both lanes
 constexpr uint32_t H2_P127 = 0x57f057f0u;   // +127.0
@@ -186,12 +190,24 @@ __device__ __forceinline__ void oms_layer(const OmsTables& tb, uint32_t* Ps, uin
             addr[j] = S::addr(tb, e, t, gbase);
             uint32_t Q = hsub2(Ps[addr[j]], get_r<S>(R, k, e));
             Q = hmin2(hmax2(Q, H2_M128), H2_P127);
-            const uint32_t a = abs_q<BETA0>(Q);
-            mn2 = hmin2(mn2, hmax2(mn1, a));
-            mn1 = hmin2(mn1, a);
+            if (BETA0) {
+                const uint32_t a = abs_q<BETA0>(Q);
+                mn2 = hmin2(mn2, hmax2(mn1, a));
+                mn1 = hmin2(mn1, a);
+                sx ^= Q;
+            } else {
+                // magnitudes as above; mn1's sign bits accumulate the sign
+                // product (Q is never -0: P and R start at +0 and x - x = +0)
+                mn2 = hmin2_xs(mn2, hmax2_xs(mn1, Q));
+                mn1 = hmin2_xs(mn1, Q);
+            }
             q[j] = Q;
-            sx ^= Q;
         }
+    }
+    if (!BETA0) {
+        sx = mn1;
+        mn1 = habs2(mn1);
+        mn2 = habs2(mn2);
     }
     const uint32_t c1 = hmin2(hmax2(hsub2(mn1, k.beta2), H2_ZERO), k.maxv2);
     const uint32_t c2 = hmin2(hmax2(hsub2(mn2, k.beta2), H2_ZERO), k.maxv2);
@@ -255,6 +271,28 @@ __device__ __forceinline__ void oms_syndrome(std::integer_sequence<int, ls...>, 
     uint32_t seen = 0;
     bool stop = false;
     (oms_syndrome_step<S, ls>(tb, Ps, t, gbase, synd, seen, stop), ...);
+}
+
+// The same syndrome as a loop over the parameter-block tables: more
+// instructions per edge, much less code (the unrolled form is a large share
+// of the kernel's instruction footprint).
+template <class S>
+__device__ __forceinline__ void oms_syndrome_loop(const OmsTables& tb, const uint32_t* Ps, int t, int gbase, uint32_t* synd) {
+    uint32_t seen = 0;
+    int e0 = 0;
+    for (int l = 0; l < tb.L; ++l) {
+        const int d = tb.rw[l];
+        const int base = S::fixed ? e0 : l * tb.D;
+        uint32_t x = 0;
+        for (int j = 0; j < d; ++j) x ^= Ps[gbase + tb.colz[base + j] + wrap_add(t, tb.shift[base + j], tb.z)];
+        e0 += d;
+        x &= 0x80008000u;
+        if (x & ~seen) {
+            atomicOr(synd, x);
+            seen |= x;
+        }
+        if (((seen | *reinterpret_cast<volatile uint32_t*>(synd)) & 0x80008000u) == 0x80008000u) break;
+    }
 }
 
 // ---- asynchronous global -> shared copies (prefetch of the next codeword) ----
@@ -369,7 +407,10 @@ __global__ void __launch_bounds__(MAXT, MINB) oms_f16_kernel(const __grid_consta
         if (tid == 0) s_busy[par ^ 1] = 0;
 
         // ================= syndrome of every slot =================
-        if (active) oms_syndrome<S>(std::make_integer_sequence<int, S::L>(), tb, Ps, t_it, gbase_it, &s_synd[par][g]);
+        if (active) {
+            if (job.synd_loop) oms_syndrome_loop<S>(tb, Ps, t_it, gbase_it, &s_synd[par][g]);
+            else oms_syndrome<S>(std::make_integer_sequence<int, S::L>(), tb, Ps, t_it, gbase_it, &s_synd[par][g]);
+        }
         __syncthreads();
 
         // ====== each warp: its slots -- decide, write out, promote, claim, prefetch ======

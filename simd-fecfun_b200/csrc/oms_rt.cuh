@@ -37,13 +37,23 @@ __device__ __forceinline__ void rt_layer(const RtCode& C, int l, uint32_t* Ps, u
             addr[j] = gbase + (int)(ed >> 9) + wrap_add(t, (int)(ed & 511u), z);
             uint32_t Q = hsub2(Ps[addr[j]], Rt[(eb + j) * nthr]);
             Q = hmin2(hmax2(Q, H2_M128), H2_P127);
-            uint32_t a = habs2(Q);
-            if (QUIRK) a = hfma2(heq2(Q, H2_M128), quirk, a);
-            mn2 = hmin2(mn2, hmax2(mn1, a));
-            mn1 = hmin2(mn1, a);
+            if (QUIRK) {
+                uint32_t a = habs2(Q);
+                a = hfma2(heq2(Q, H2_M128), quirk, a);
+                mn2 = hmin2(mn2, hmax2(mn1, a));
+                mn1 = hmin2(mn1, a);
+                sx ^= Q;
+            } else {
+                mn2 = hmin2_xs(mn2, hmax2_xs(mn1, Q));   // as oms_layer: signs ride in mn1
+                mn1 = hmin2_xs(mn1, Q);
+            }
             q[j] = Q;
-            sx ^= Q;
         }
+    }
+    if (!QUIRK) {
+        sx = mn1;
+        mn1 = habs2(mn1);
+        mn2 = habs2(mn2);
     }
     const uint32_t c1 = hmin2(hmax2(hsub2(mn1, beta2), H2_ZERO), C.maxv2);
     const uint32_t c2 = hmin2(hmax2(hsub2(mn2, beta2), H2_ZERO), C.maxv2);

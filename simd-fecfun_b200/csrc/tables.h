@@ -35,6 +35,7 @@ struct OmsJob {
     uint32_t maxv2;                  // half2 bits of Max8
     unsigned long long* queue;       // work counter, zero before launch
     unsigned int* status;            // error word (0 = ok)
+    int synd_loop;                   // 1: syndrome as a loop over the parameter tables (smaller code)
 };
 
 // ---- float decoders (sum-product / offset min-sum), R in shared memory ----
