@@ -229,11 +229,14 @@ def run_workload(args):
     torch.cuda.set_device(local)
     clk = _clock_sampler(local)
     if args.workload == "nr-mix":
-        out = workloads.nr_mix(steps=args.steps, warmup=args.warmup)
+        out = workloads.nr_mix(steps=args.steps, warmup=args.warmup, llr_budget=args.llr_budget_gb * 1e9,
+                               autotune=not args.no_autotune)
     elif args.workload == "hetero-mix":
         out = workloads.hetero_mix(steps=args.steps, warmup=args.warmup)
+    elif args.workload == "sp-sweep":
+        out = workloads.sp_sweep(cw_per_z=args.sp_cw)
     else:
-        out = workloads.learned_run(train_steps=max(args.steps, 5))
+        out = workloads.learned_run(train_steps=max(args.steps, 2), batch=args.learned_batch)
     out["clocks"] = _clock_summary(clk)
     print(json.dumps(out), flush=True)
     return 0
@@ -251,9 +254,14 @@ def main():
     ap.add_argument("--cpu-reps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="11ad", choices=["11ad", "nr-mix", "hetero-mix", "learned"],
+    ap.add_argument("--workload", default="11ad", choices=["11ad", "nr-mix", "hetero-mix", "learned", "sp-sweep"],
                     help="11ad: the headline run; others: the batched 5G NR mix, the 18-code 802.11 mix "
-                         "(plain vs learned offsets), learned-offset training (one GPU)")
+                         "(plain vs learned offsets), learned-offset training, the float sum-product Z sweep "
+                         "(one GPU)")
+    ap.add_argument("--llr-budget-gb", type=float, default=40.0, help="nr-mix: LLR bytes the codeword counts are scaled to")
+    ap.add_argument("--no-autotune", action="store_true", help="nr-mix: default launch shape")
+    ap.add_argument("--learned-batch", type=int, default=65536)
+    ap.add_argument("--sp-cw", type=int, default=1 << 20, help="sp-sweep: codewords per Z")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

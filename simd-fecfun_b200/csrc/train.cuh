@@ -177,6 +177,22 @@ __global__ void __launch_bounds__(512) oms_train_fwd(const __grid_constant__ SpT
     }
 }
 
+// Global -> shared copy of m floats: 16-byte vector loads, several in flight
+// per thread, when both ends are 16-byte aligned and m % 4 == 0.
+__device__ __forceinline__ void tr_copy(float* dst, const float* src, int m) {
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    if (((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0 && (m & 3) == 0) {
+        const float4* s4 = reinterpret_cast<const float4*>(src);
+        float4* d4 = reinterpret_cast<float4*>(dst);
+        const int m4 = m >> 2;
+#pragma unroll 8
+        for (int i = tid; i < m4; i += nthr) d4[i] = __ldg(s4 + i);
+    } else {
+#pragma unroll 8
+        for (int i = tid; i < m; i += nthr) dst[i] = __ldg(src + i);
+    }
+}
+
 // deterministic block sum of v (fixed reduction order); all threads must call
 __device__ __forceinline__ float tr_block_sum(float v, float* red) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -215,6 +231,7 @@ __global__ void __launch_bounds__(512) oms_train_bwd(const __grid_constant__ SpT
             // 1. loss adjoint at the end of iteration it
             const float* pe = job.ckpt_p + ((long long)(it + 1) * job.ncw + cw) * n;
             const float wk = job.loss_w[it] * job.inv_norm;
+#pragma unroll 4
             for (int i = tid; i < n; i += nthr) {
                 const float s = bits[i] ? -1.0f : 1.0f;
                 const float x = -s * pe[i];
@@ -224,8 +241,8 @@ __global__ void __launch_bounds__(512) oms_train_bwd(const __grid_constant__ SpT
             // 2. reload the checkpoint and recompute the layers, keeping Q
             const float* cp = job.ckpt_p + ((long long)it * job.ncw + cw) * n;
             const float* cr = job.ckpt_r + ((long long)it * job.ncw + cw) * EZ;
-            for (int i = tid; i < n; i += nthr) P[i] = cp[i];
-            for (int i = tid; i < EZ; i += nthr) QR[i] = cr[i];
+            tr_copy(P, cp, n);
+            tr_copy(QR, cr, EZ);
             __syncthreads();
             for (int l = 0; l < L; ++l) {
                 if (active) tr_layer<DMAX>(tb, l, P, QR, t, job.beta[it * L + l], job.maxv, true);

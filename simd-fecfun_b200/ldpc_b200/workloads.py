@@ -14,6 +14,8 @@
   (802.16e 1/2, Z=96, 10 iterations x 12 layers, batches of 65536
   codewords), then codeword error rate and average iterations of learned
   vs plain offsets.
+* :func:`sp_sweep` -- float sum-product on 802.16e 1/2 for all 19 lifting
+  sizes Z = 24..96.
 
 Inputs are synthetic, drawn on the device by the library's generator
 (Philox data bits, QC encoding, AWGN); SNRs given as Eb/N0 are converted to
@@ -87,7 +89,8 @@ def _time_plan(plan, specs, steps, warmup, graph=True):
     return [a.elapsed_time(b) for a, b in ev]
 
 
-def nr_mix(steps: int = 3, warmup: int = 1, seed: int = 7, llr_budget: float = 40e9, ebn0=(0.5, 1.0, 1.5)) -> Dict:
+def nr_mix(steps: int = 3, warmup: int = 1, seed: int = 7, llr_budget: float = 40e9, ebn0=(0.5, 1.0, 1.5),
+           autotune: bool = True) -> Dict:
     names = ["5GNR_n25344_k8448", "5GNR_n3136_k576", "5GNR_n6400_k1280", "5GNR_n12800_k2560"]
     objs = [codes.code_by_name(n) for n in names]
     rng = np.random.default_rng(seed)
@@ -100,7 +103,7 @@ def nr_mix(steps: int = 3, warmup: int = 1, seed: int = 7, llr_budget: float = 4
     specs, meta = _build_jobs(handles, objs, counts, snrs, seed, 20)
     batch = capi.Batch(handles, [dict(max_iter=20)] * len(objs))
     t0 = time.time()
-    tuned = batch.autotune(specs, sample=16384)
+    tuned = batch.autotune(specs, sample=16384) if autotune else (0, 0, 0.0)
     tune_s = time.time() - t0
     plan = batch.plan(specs)
     ms = _time_plan(plan, specs, steps, warmup)
@@ -228,7 +231,7 @@ def hetero_mix(steps: int = 3, warmup: int = 1, total: int = 10_000_000, seed: i
 
 
 def learned_run(train_steps: int = 30, batch: int = 65536, eval_n: int = 200_000, seed: int = 3) -> Dict:
-    code = codes.make_code("16e 1/2")
+    code = codes.make_code("16e 1/2", z_over=96)
     h = capi.Code.from_tables(code)
     ctx = capi.Context(h, variant=capi.LDPC_F32_OMS, max_iter=10, max_row_metric=31.0, beta=0.5, llr_scale=1.0,
                        max_abs_llr=1e9)
@@ -279,4 +282,59 @@ def learned_run(train_steps: int = 30, batch: int = 65536, eval_n: int = 200_000
         "offsets": [[round(float(v), 3) for v in row] for row in beta.cpu()],
         "evaluation": evals,
         "gpu_launches": None,
+    }
+
+
+def sp_sweep(cw_per_z: int = 1 << 20, ebn0=(0.5, 1.0, 1.5, 2.0), seed: int = 5, max_iter: int = 10) -> Dict:
+    """802.16e rate 1/2 for every Z = 24, 28, ..., 96 (N = 576..2304), float
+    sum-product (clamp 1 - 6e-8, LLR = 2y/sigma^2, no LLR limit), 10
+    iterations.  Each Z's codewords (spread over the Eb/N0 points) are drawn
+    on the device, then decoded with fused counting in one launch per Z; the
+    decode launches are timed."""
+    zs = list(range(24, 97, 4))
+    s = torch.cuda.current_stream()
+    total_ms, total_cw, info_bits = 0.0, 0, 0
+    quality = []
+    for z in zs:
+        c = codes.make_code("16e 1/2", z_over=z)
+        h = capi.Code.from_tables(c)
+        ctx = capi.Context(h, variant=capi.LDPC_F32_SP, max_iter=max_iter, max_row_metric=6e-8, beta=0.0,
+                           llr_scale=1.0, max_abs_llr=1e9)
+        k = len(ebn0)
+        per = cw_per_z // k
+        llr = torch.empty((k, per, c.n), dtype=torch.float32, device="cuda")
+        data = torch.empty((k, per, h.info.hard_words), dtype=torch.int32, device="cuda")
+        for i, e in enumerate(ebn0):
+            ctx.generate(seed + z, i * per, [learned.snr_from_ebn0(e, 0.5)], per, llr_f32=llr[i:i + 1],
+                         data_bits=data[i], stream=s.cuda_stream)
+        cnt = torch.zeros((k, 4), dtype=torch.int64, device="cuda")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(s)
+        for i in range(k):
+            ctx.decode_count(llr[i], per, data_bits=data[i], ref_period=per, bucket_size=per, counters=cnt[i:i + 1],
+                             n_buckets=1, stream=s.cuda_stream)
+        e1.record(s)
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        total_cw += k * per
+        info_bits += k * per * c.k
+        cc = cnt.cpu().numpy()
+        for i, e in enumerate(ebn0):
+            quality.append(dict(z=z, ebn0_db=e, codewords=int(cc[i, 0]), avg_iter=float(cc[i, 1]) / max(1, cc[i, 0]),
+                                cwer=float(cc[i, 3]) / max(1, cc[i, 0])))
+        del llr, data, ctx
+    return {
+        "metric": "codewords/s decoded, 802.16e 1/2 Z=24..96 (19 sizes), float32 layered sum-product, 10 max iterations",
+        "value": total_cw / (total_ms * 1e-3), "unit": "codewords/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+        "ms_per_step": total_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: Philox data bits, QC encoding, AWGN from the fused generator, resident in HBM",
+        "config": {"workload": "802.16e 1/2, Z in 24..96 step 4 (shifts mod Z), %d codewords per Z over Eb/N0 %s dB "
+                               "(Es/N0 = Eb/N0 - 3.01 dB), sum-product clamp 1-6e-8, LLR scale 1, no LLR limit"
+                               % (cw_per_z, list(ebn0)),
+                   "launch": "one ldpc_decode_count launch per (Z, Eb/N0) block; the float decoders have no multi-code "
+                             "launch"},
+        "info_gbps": info_bits / (total_ms * 1e-3) / 1e9,
+        "gpu_launches": len(zs) * len(ebn0),
+        "quality": quality,
     }

@@ -87,7 +87,7 @@ def test_contexts_sharing_a_kernel_keep_their_shared_memory(capi, oracle):
     shared-memory sizes: creating the smaller one must not break launches of
     the larger one (the limit belongs to the kernel, not to a context)."""
     from ldpc_b200 import codes
-    big = codes.make_code("16e 1/2")
+    big = codes.make_code("16e 1/2", z_over=96)
     small = codes.make_code("16e 1/2", z_over=24)
     kw = dict(variant=capi.LDPC_F32_SP, max_iter=10, max_row_metric=6e-8, beta=0.0, llr_scale=1.0, max_abs_llr=1e9)
     ctx_big = capi.Context(capi.Code.from_tables(big), **kw)

@@ -29,7 +29,7 @@ def _data(oracle, code, n, sigma, seed):
     return llr, cw
 
 
-@pytest.mark.parametrize("name,zo,sigma", [("16e 1/2", 24, 0.85), ("16e 1/2", None, 0.8), ("11n 2/3 z27", None, 0.7)])
+@pytest.mark.parametrize("name,zo,sigma", [("16e 1/2", 24, 0.85), ("16e 1/2", 96, 0.8), ("11n 2/3 z27", None, 0.7)])
 def test_constant_offsets_equal_float_min_sum(capi, oracle, name, zo, sigma):
     import torch
     from ldpc_b200 import codes
@@ -116,12 +116,12 @@ def test_adjoint_matches_fp64_autograd_and_finite_differences(capi, oracle):
     assert np.abs(g_cuda - fd4)[smooth].max() <= GRAD_TOL * scale + FD_TOL * scale
 
 
-@pytest.mark.parametrize("n,iters,zo", [(16, 5, 24), (16, 10, None)])
+@pytest.mark.parametrize("n,iters,zo", [(16, 5, 24), (16, 10, 96)])
 def test_adjoint_matches_fp64_autograd(capi, oracle, n, iters, zo):
     """Larger cases against the fp64 autograd gradient; Z=96 (N=2304) with
     10 iterations x 12 layers = 120 offsets."""
     from ldpc_b200 import codes
-    code = codes.make_code("16e 1/2", z_over=zo) if zo else codes.make_code("16e 1/2")
+    code = codes.make_code("16e 1/2", z_over=zo)
     ctx, llr, cw, b0, w, loss, g_cuda, ref, g_ref, tables = _grads(capi, oracle, code, n, iters, 0.8, 5)
     assert abs(loss - ref) <= 1e-4 * abs(ref)
     assert np.abs(g_cuda - g_ref).max() <= GRAD_TOL * np.abs(g_ref).max()
@@ -130,7 +130,7 @@ def test_adjoint_matches_fp64_autograd(capi, oracle, n, iters, zo):
 def test_gradient_is_deterministic(capi, oracle):
     import torch
     from ldpc_b200 import codes, learned
-    code = codes.make_code("16e 1/2")
+    code = codes.make_code("16e 1/2", z_over=96)
     ctx = _ctx(capi, code)
     llr, cw = _data(oracle, code, 700, 0.8, 7)
     d, bits = torch.from_numpy(llr).cuda(), torch.from_numpy(cw).cuda()
@@ -147,7 +147,7 @@ def test_training_lowers_the_loss(capi):
     """Offsets trained from 0 lower the loss on a fixed held-out batch."""
     import torch
     from ldpc_b200 import codes, learned
-    code = codes.make_code("16e 1/2")
+    code = codes.make_code("16e 1/2", z_over=96)
     ctx = _ctx(capi, code)
     beta, hist = learned.train(ctx, code, iters=6, batch=2048, steps=30, lr=0.05, init=0.0, seed=2)
     assert beta.shape == (6, code.mrow) and float(beta.min()) >= 0.0
