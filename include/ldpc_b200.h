@@ -43,7 +43,9 @@ enum {
 enum {
     LDPC_INT8_OMS = 0,          /* int8 offset min-sum   (LDPCtop_Vec64c_min)  */
     LDPC_F32_SP = 1,            /* float sum-product     (LDPCtop_Vec16f_prod) */
-    LDPC_F32_OMS = 2            /* float offset min-sum  (LDPCtop_Vec16f_min)  */
+    LDPC_F32_OMS = 2,           /* float offset min-sum  (LDPCtop_Vec16f_min)  */
+    LDPC_INT16_OMS = 3,         /* int16 offset min-sum  (LDPCtop_Vec32s_min)  */
+    LDPC_INT32_OMS = 4          /* int32 offset min-sum  (LDPCtop_Vec16w_min)  */
 };
 
 typedef struct ldpc_code ldpc_code;
@@ -65,10 +67,10 @@ typedef struct {
  * (sim_struct_LDPC.h:3-20) plus the variant, which the reference selects at
  * compile time (build/Makefile:9-14). */
 typedef struct {
-    int variant;                /* LDPC_INT8_OMS / LDPC_F32_SP / LDPC_F32_OMS */
+    int variant;                /* LDPC_INT8_OMS / LDPC_F32_SP / LDPC_F32_OMS / LDPC_INT16_OMS / LDPC_INT32_OMS */
     unsigned max_iter;          /* maximum decoder iterations (1..255) */
     float max_row_metric;       /* min-sum clamp, or 1-clamp for sum-product */
-    float beta;                 /* offset (truncated to an integer for int8) */
+    float beta;                 /* offset (truncated to the element type for the integer variants) */
     float llr_scale;            /* LLR_scaling_factor */
     float max_abs_llr;          /* max_abs_LLR */
 } ldpc_cfg;
@@ -120,7 +122,16 @@ int ldpc_decode_int8(ldpc_ctx *ctx, const int8_t *llr, size_t n, int8_t *post_ou
 int ldpc_decode_f32(ldpc_ctx *ctx, const float *llr, size_t n, float *post_out, uint32_t *hard_out,
                     uint8_t *iters_out, void *stream);
 
-/* Decode with fused error counting (either variant; dev pointers, async).
+/* int16 / int32 decoders (LDPC_INT16_OMS / LDPC_INT32_OMS): same contract,
+ * LLRs and posteriors of the element type.  The reference's element
+ * semantics hold: saturating add/sub, abs of the most negative value is
+ * itself, beta and max_row_metric truncated to the element type. */
+int ldpc_decode_int16(ldpc_ctx *ctx, const int16_t *llr, size_t n, int16_t *post_out, uint32_t *hard_out,
+                      uint8_t *iters_out, void *stream);
+int ldpc_decode_int32(ldpc_ctx *ctx, const int32_t *llr, size_t n, int32_t *post_out, uint32_t *hard_out,
+                      uint8_t *iters_out, void *stream);
+
+/* Decode with fused error counting (any variant; dev pointers, async).
  * Codeword i is compared with sent data bits data_bits[i % ref_period] and
  * counted in bucket min(i / bucket_size, n_buckets-1) of
  * counters[n_buckets][4] = {codewords, iterations, bit errors, codeword
@@ -138,12 +149,16 @@ int ldpc_decode_int8_host(ldpc_ctx *ctx, const int8_t *llr, size_t n, int8_t *po
                           uint8_t *iters_out, uint64_t *tot_iter);
 int ldpc_decode_f32_host(ldpc_ctx *ctx, const float *llr, size_t n, float *post_out, uint32_t *hard_out,
                          uint8_t *iters_out, uint64_t *tot_iter);
+int ldpc_decode_int16_host(ldpc_ctx *ctx, const int16_t *llr, size_t n, int16_t *post_out, uint32_t *hard_out,
+                           uint8_t *iters_out, uint64_t *tot_iter);
+int ldpc_decode_int32_host(ldpc_ctx *ctx, const int32_t *llr, size_t n, int32_t *post_out, uint32_t *hard_out,
+                           uint8_t *iters_out, uint64_t *tot_iter);
 
 /* Literal drop-in for LDPCdecode_set (LDPCdecode.cpp:203-245): decodes, in
  * place, num_codeword codewords stored in the reference's padded host layout
  * -- per codeword mcol columns of (ceil(Z/simd_par)+2)*simd_par elements,
  * element t of column c at offset simd_par + t (decode_matrix_allocate.cpp:55)
- * -- with int8 elements for LDPC_INT8_OMS and float for the float variants.
+ * -- with elements of the variant's type (int8, int16, int32 or float).
  * *tot_iter receives the sum of iterations. */
 int ldpc_decode_set_compat(ldpc_ctx *ctx, void *decoded_metrics, unsigned num_codeword, unsigned simd_par,
                            uint64_t *tot_iter);

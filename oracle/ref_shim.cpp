@@ -53,9 +53,18 @@ void *ref_open(const char *enc_path, const char *dec_path, unsigned num_cw) {
     encode_matrix_allocate(enc_path, &c->enc, num_cw);
     decode_matrix_allocate(dec_path, &c->dec, num_cw);
     c->num_cw = num_cw;
-    /* zero the codeword and metric buffers (the reference leaves them uninitialised) */
+    /* The reference's mirror copies (LDPCdecode.cpp:133-150) store whole SIMD
+     * words at unaligned offsets, and the last one of the buffer can end past
+     * the allocation of decode_matrix_allocate.cpp:55 (seen with the int16
+     * build at Z=24: 2 bytes over).  Decode into a copy with two spare
+     * columns behind it, so such a store lands in slack instead of the heap. */
     unsigned spz = (c->dec.z_value + SIMD_PAR - 1) / SIMD_PAR;
-    memset(c->dec.decoded_metrics, 0, (size_t)num_cw * c->dec.mcol * (spz + 2) * (WIDTH / 8));
+    const size_t bytes = (size_t)num_cw * c->dec.mcol * (spz + 2) * (WIDTH / 8);
+    const size_t slack = (size_t)2 * (spz + 2) * (WIDTH / 8);
+    _mm_free(c->dec.decoded_metrics);
+    c->dec.decoded_metrics = (SIMD_CLASS *)_mm_malloc(bytes + slack, WIDTH / 8);
+    /* zero the codeword and metric buffers (the reference leaves them uninitialised) */
+    memset(c->dec.decoded_metrics, 0, bytes + slack);
     memset(c->enc.cw_bits, 0, (size_t)num_cw * c->enc.mcol * sizeof(ENC_CLASS));
     return c;
 }

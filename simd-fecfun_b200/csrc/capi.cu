@@ -245,6 +245,15 @@ void ldpc_code_destroy(ldpc_code* c) { delete c; }
 // ---------------------------------------------------------------------------
 namespace ldpc {
 
+int launch_decode(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s) {
+    switch (x->cfg.variant) {
+        case LDPC_INT8_OMS: return launch_oms(x, a, s);
+        case LDPC_INT16_OMS:
+        case LDPC_INT32_OMS: return launch_int(x, a, s);
+        default: return launch_sp(x, a, s);
+    }
+}
+
 int8_t max_row_i8(float m) {
     // decode_row's Max_row_simd for an int8 build (decode_functions.cpp:27-32)
     if (m < 1e-6) return (int8_t)(1.0 - (double)(int8_t)m);
@@ -260,7 +269,7 @@ int ldpc_ctx_create(const ldpc_code* code, const ldpc_cfg* cfg, int device, ldpc
     *out = nullptr;
     if (cfg->max_iter < 1 || cfg->max_iter > 255)
         return fail(LDPC_ERR_UNSUPPORTED, "max_iter=%u outside 1..255", cfg->max_iter);
-    if (cfg->variant != LDPC_INT8_OMS && cfg->variant != LDPC_F32_SP && cfg->variant != LDPC_F32_OMS)
+    if (cfg->variant < LDPC_INT8_OMS || cfg->variant > LDPC_INT32_OMS)
         return fail(LDPC_ERR_INVALID_ARG, "unknown variant %d", cfg->variant);
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -293,6 +302,9 @@ int ldpc_ctx_create(const ldpc_code* code, const ldpc_cfg* cfg, int device, ldpc
         x->maxv2 = ldpc::half2_bits((float)max8);
         int rc = ldpc::setup_oms(x.get());
         if (rc) return rc;
+    } else if (cfg->variant == LDPC_INT16_OMS || cfg->variant == LDPC_INT32_OMS) {
+        int rc = ldpc::setup_int(x.get());
+        if (rc) return rc;
     } else {
         int rc = ldpc::setup_sp(x.get());
         if (rc) return rc;
@@ -321,6 +333,7 @@ void ldpc_ctx_destroy(ldpc_ctx* x) {
     cudaFree(x->d_status);
     cudaFree(x->d_counters);
     cudaFree(x->d_sp_scratch);
+    cudaFree(x->d_int_scratch);
     cudaFree(x->d_rt_code);
     cudaFree(x->d_rt_scratch);
     for (int i = 0; i < 2; ++i) {
@@ -337,13 +350,17 @@ void ldpc_ctx_destroy(ldpc_ctx* x) {
 
 namespace {
 
-int check_decode_args(ldpc_ctx* x, size_t n, const void* llr, int want_variant_int8) {
+// LLR element kinds of the entry points: 0 int8, 1 float, 2 int16, 3 int32
+int llr_kind(int variant) {
+    return variant == LDPC_INT8_OMS ? 0 : variant == LDPC_INT16_OMS ? 2 : variant == LDPC_INT32_OMS ? 3 : 1;
+}
+
+int check_decode_args(ldpc_ctx* x, size_t n, const void* llr, int kind) {
+    static const char* names[] = {"int8", "float", "int16", "int32"};
     if (!x) return fail(LDPC_ERR_INVALID_ARG, "ctx is NULL");
     if (n && !llr) return fail(LDPC_ERR_INVALID_ARG, "llr is NULL");
-    const bool is8 = x->cfg.variant == LDPC_INT8_OMS;
-    if (want_variant_int8 != (int)is8)
-        return fail(LDPC_ERR_INVALID_ARG, "context variant %d does not take %s LLRs", x->cfg.variant,
-                    want_variant_int8 ? "int8" : "float");
+    if (llr_kind(x->cfg.variant) != kind)
+        return fail(LDPC_ERR_INVALID_ARG, "context variant %d does not take %s LLRs", x->cfg.variant, names[kind]);
     if (n > (size_t)1 << 40) return fail(LDPC_ERR_INVALID_ARG, "n=%zu too large", n);
     return LDPC_OK;
 }
@@ -405,7 +422,7 @@ int decode_host(ldpc_ctx* x, const T* llr, size_t n, T* post, uint32_t* hard, ui
         a.hard = (uint32_t*)d_hard;
         a.iters = (uint8_t*)d_it;
         a.queue = b;
-        rc = (x->cfg.variant == LDPC_INT8_OMS) ? ldpc::launch_oms(x, a, s) : ldpc::launch_sp(x, a, s);
+        rc = ldpc::launch_decode(x, a, s);
         if (rc) break;
         if ((post && cudaMemcpyAsync(post + off * N, d_post, m * N * sizeof(T), cudaMemcpyDeviceToHost, s)) ||
             (hard && cudaMemcpyAsync(hard + off * HW, d_hard, m * HW * 4, cudaMemcpyDeviceToHost, s)) ||
@@ -432,7 +449,7 @@ extern "C" {
 
 int ldpc_decode_int8(ldpc_ctx* x, const int8_t* llr, size_t n, int8_t* post_out, uint32_t* hard_out,
                      uint8_t* iters_out, void* stream) {
-    int rc = check_decode_args(x, n, llr, 1);
+    int rc = check_decode_args(x, n, llr, 0);
     if (rc) return rc;
     CUDA_TRY(cudaSetDevice(x->device));
     ldpc::DecodeArgs a;
@@ -446,7 +463,7 @@ int ldpc_decode_int8(ldpc_ctx* x, const int8_t* llr, size_t n, int8_t* post_out,
 
 int ldpc_decode_f32(ldpc_ctx* x, const float* llr, size_t n, float* post_out, uint32_t* hard_out, uint8_t* iters_out,
                     void* stream) {
-    int rc = check_decode_args(x, n, llr, 0);
+    int rc = check_decode_args(x, n, llr, 1);
     if (rc) return rc;
     CUDA_TRY(cudaSetDevice(x->device));
     ldpc::DecodeArgs a;
@@ -477,22 +494,63 @@ int ldpc_decode_count(ldpc_ctx* x, const void* llr, size_t n, uint32_t* hard_out
     a.bucket_size = bucket_size ? (long long)bucket_size : (long long)n;
     a.counters = counters;
     a.n_buckets = n_buckets;
-    return x->cfg.variant == LDPC_INT8_OMS ? ldpc::launch_oms(x, a, (cudaStream_t)stream)
-                                           : ldpc::launch_sp(x, a, (cudaStream_t)stream);
+    return ldpc::launch_decode(x, a, (cudaStream_t)stream);
 }
 
 int ldpc_decode_int8_host(ldpc_ctx* x, const int8_t* llr, size_t n, int8_t* post_out, uint32_t* hard_out,
                           uint8_t* iters_out, uint64_t* tot_iter) {
-    int rc = check_decode_args(x, n, llr, 1);
+    int rc = check_decode_args(x, n, llr, 0);
     if (rc) return rc;
     return decode_host<int8_t>(x, llr, n, post_out, hard_out, iters_out, tot_iter);
 }
 
 int ldpc_decode_f32_host(ldpc_ctx* x, const float* llr, size_t n, float* post_out, uint32_t* hard_out,
                          uint8_t* iters_out, uint64_t* tot_iter) {
-    int rc = check_decode_args(x, n, llr, 0);
+    int rc = check_decode_args(x, n, llr, 1);
     if (rc) return rc;
     return decode_host<float>(x, llr, n, post_out, hard_out, iters_out, tot_iter);
+}
+
+int ldpc_decode_int16(ldpc_ctx* x, const int16_t* llr, size_t n, int16_t* post_out, uint32_t* hard_out,
+                      uint8_t* iters_out, void* stream) {
+    int rc = check_decode_args(x, n, llr, 2);
+    if (rc) return rc;
+    CUDA_TRY(cudaSetDevice(x->device));
+    ldpc::DecodeArgs a;
+    a.llr = llr;
+    a.n = n;
+    a.post = post_out;
+    a.hard = hard_out;
+    a.iters = iters_out;
+    return ldpc::launch_int(x, a, (cudaStream_t)stream);
+}
+
+int ldpc_decode_int32(ldpc_ctx* x, const int32_t* llr, size_t n, int32_t* post_out, uint32_t* hard_out,
+                      uint8_t* iters_out, void* stream) {
+    int rc = check_decode_args(x, n, llr, 3);
+    if (rc) return rc;
+    CUDA_TRY(cudaSetDevice(x->device));
+    ldpc::DecodeArgs a;
+    a.llr = llr;
+    a.n = n;
+    a.post = post_out;
+    a.hard = hard_out;
+    a.iters = iters_out;
+    return ldpc::launch_int(x, a, (cudaStream_t)stream);
+}
+
+int ldpc_decode_int16_host(ldpc_ctx* x, const int16_t* llr, size_t n, int16_t* post_out, uint32_t* hard_out,
+                           uint8_t* iters_out, uint64_t* tot_iter) {
+    int rc = check_decode_args(x, n, llr, 2);
+    if (rc) return rc;
+    return decode_host<int16_t>(x, llr, n, post_out, hard_out, iters_out, tot_iter);
+}
+
+int ldpc_decode_int32_host(ldpc_ctx* x, const int32_t* llr, size_t n, int32_t* post_out, uint32_t* hard_out,
+                           uint8_t* iters_out, uint64_t* tot_iter) {
+    int rc = check_decode_args(x, n, llr, 3);
+    if (rc) return rc;
+    return decode_host<int32_t>(x, llr, n, post_out, hard_out, iters_out, tot_iter);
 }
 
 int ldpc_decode_set_compat(ldpc_ctx* x, void* metrics, unsigned num_cw, unsigned simd_par, uint64_t* tot_iter) {
@@ -502,16 +560,20 @@ int ldpc_decode_set_compat(ldpc_ctx* x, void* metrics, unsigned num_cw, unsigned
     const size_t spz = (z + simd_par - 1) / simd_par;
     const size_t col = (spz + 2) * simd_par;   // elements per column incl. the two pad words
     const size_t N = (size_t)x->n;
-    const bool is8 = x->cfg.variant == LDPC_INT8_OMS;
-    const size_t es = is8 ? 1 : 4;
+    const size_t es = (size_t)ldpc::llr_bytes(x->cfg.variant);
     std::vector<uint8_t> flat(num_cw * N * es), post(num_cw * N * es);
     uint8_t* m = (uint8_t*)metrics;
     for (size_t w = 0; w < num_cw; ++w)
         for (int c = 0; c < mcol; ++c)
             memcpy(&flat[(w * N + (size_t)c * z) * es], m + ((w * mcol + c) * col + simd_par) * es, (size_t)z * es);
     uint64_t it = 0;
-    int rc = is8 ? decode_host<int8_t>(x, (const int8_t*)flat.data(), num_cw, (int8_t*)post.data(), nullptr, nullptr, &it)
-                 : decode_host<float>(x, (const float*)flat.data(), num_cw, (float*)post.data(), nullptr, nullptr, &it);
+    int rc;
+    switch (llr_kind(x->cfg.variant)) {
+        case 0: rc = decode_host<int8_t>(x, (const int8_t*)flat.data(), num_cw, (int8_t*)post.data(), nullptr, nullptr, &it); break;
+        case 2: rc = decode_host<int16_t>(x, (const int16_t*)flat.data(), num_cw, (int16_t*)post.data(), nullptr, nullptr, &it); break;
+        case 3: rc = decode_host<int32_t>(x, (const int32_t*)flat.data(), num_cw, (int32_t*)post.data(), nullptr, nullptr, &it); break;
+        default: rc = decode_host<float>(x, (const float*)flat.data(), num_cw, (float*)post.data(), nullptr, nullptr, &it);
+    }
     if (rc) return rc;
     for (size_t w = 0; w < num_cw; ++w)
         for (int c = 0; c < mcol; ++c)

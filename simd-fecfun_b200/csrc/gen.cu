@@ -82,6 +82,8 @@ int launch_gen(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* snr_
                int8_t* llr_i8, float* llr_f32, uint32_t* data_bits, unsigned long long* uncoded, cudaStream_t s) {
     if (!x->code.has_enc) return fail(LDPC_ERR_INVALID_ARG, "code has no encoder table");
     if (!x->gen_ok) return fail(LDPC_ERR_UNSUPPORTED, "generator: %s", x->gen_err.c_str());
+    if (x->cfg.variant == LDPC_INT16_OMS || x->cfg.variant == LDPC_INT32_OMS)
+        return fail(LDPC_ERR_UNSUPPORTED, "generator: int16/int32 LLRs are not produced on the device");
     if (n_snr < 1 || n_snr > (size_t)GEN_MAX_SNR) return fail(LDPC_ERR_INVALID_ARG, "n_snr=%zu outside 1..%d", n_snr, GEN_MAX_SNR);
     if (!snr_db) return fail(LDPC_ERR_INVALID_ARG, "snr_db is NULL");
     if (n_per_snr == 0) return LDPC_OK;
@@ -203,7 +205,7 @@ int ldpc_simulate(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* s
             a.counters = dc + 4 * k;
             a.n_buckets = 1;
             CUDA_TRY(cudaEventRecord(x->ev_start, s));
-            rc = is8 ? ldpc::launch_oms(x, a, s) : ldpc::launch_sp(x, a, s);
+            rc = ldpc::launch_decode(x, a, s);
             if (rc) return rc;
             CUDA_TRY(cudaEventRecord(x->ev_stop, s));
             CUDA_TRY(cudaEventSynchronize(x->ev_stop));

@@ -109,6 +109,11 @@ struct ldpc_ctx {
     int sp_threads = 0, sp_smem = 0, sp_ctas = 0;
     float* d_sp_scratch = nullptr;              // check messages of large codes (global)
     float maxf = 0.f;
+    // int16 / int32 decoders (tables in spt)
+    void* int_kernel = nullptr;
+    int int_threads = 0, int_smem = 0, int_ctas = 0;
+    void* d_int_scratch = nullptr;
+    int ibeta = 0, imaxv = 0;
     // generation
     ldpc::GenTables gent;
     bool gen_ok = false;                        // generator/encoder usable for this code
@@ -146,6 +151,14 @@ rt_fn rt_kernel_for(int dmax, bool quirk, bool rsmem);
 int rt_stride(int n, int G);
 // dynamic shared memory of one CTA: tables, G pairs of posteriors and staging, messages if rsmem
 size_t rt_smem_bytes(int n, int G, int E, int threads, bool rsmem);
+int setup_int(ldpc_ctx* x);
+int launch_int(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s);
+// the decoder of the context's variant
+int launch_decode(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s);
+// bytes per LLR / posterior element of a variant
+inline int llr_bytes(int variant) {
+    return variant == LDPC_INT8_OMS ? 1 : variant == LDPC_INT16_OMS ? 2 : 4;
+}
 int setup_sp(ldpc_ctx* x);
 int launch_sp(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s);
 int setup_gen(ldpc_ctx* x);

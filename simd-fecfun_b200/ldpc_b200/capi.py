@@ -27,6 +27,8 @@ LDPC_ERR_NOMEM = 7
 LDPC_INT8_OMS = 0
 LDPC_F32_SP = 1
 LDPC_F32_OMS = 2
+LDPC_INT16_OMS = 3
+LDPC_INT32_OMS = 4
 
 ERROR_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "BAD_TABLE", 3: "UNSUPPORTED", 4: "CUDA", 5: "TIMEOUT", 6: "IO",
                7: "NOMEM"}
@@ -74,6 +76,10 @@ _PROTOS = {
     "ldpc_ctx_destroy": (None, [_vp]),
     "ldpc_decode_int8": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _vp]),
     "ldpc_decode_f32": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _vp]),
+    "ldpc_decode_int16": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _vp]),
+    "ldpc_decode_int32": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _vp]),
+    "ldpc_decode_int16_host": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, C.POINTER(C.c_uint64)]),
+    "ldpc_decode_int32_host": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, C.POINTER(C.c_uint64)]),
     "ldpc_decode_int8_host": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, C.POINTER(C.c_uint64)]),
     "ldpc_decode_f32_host": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, C.POINTER(C.c_uint64)]),
     "ldpc_decode_set_compat": (C.c_int, [_vp, _vp, C.c_uint, C.c_uint, C.POINTER(C.c_uint64)]),
@@ -215,6 +221,12 @@ class Context:
     def decode_f32(self, llr, n, post=None, hard=None, iters=None, stream=0):
         check(lib.ldpc_decode_f32(self.h, _ptr(llr), n, _ptr(post), _ptr(hard), _ptr(iters), stream or None))
 
+    def decode_int16(self, llr, n, post=None, hard=None, iters=None, stream=0):
+        check(lib.ldpc_decode_int16(self.h, _ptr(llr), n, _ptr(post), _ptr(hard), _ptr(iters), stream or None))
+
+    def decode_int32(self, llr, n, post=None, hard=None, iters=None, stream=0):
+        check(lib.ldpc_decode_int32(self.h, _ptr(llr), n, _ptr(post), _ptr(hard), _ptr(iters), stream or None))
+
     def decode_count(self, llr, n, hard=None, iters=None, data_bits=None, ref_period=1, bucket_size=0, counters=None,
                      n_buckets=1, stream=0):
         check(lib.ldpc_decode_count(self.h, _ptr(llr), n, _ptr(hard), _ptr(iters), _ptr(data_bits), ref_period,
@@ -254,9 +266,11 @@ class Context:
         hard = np.empty((n, self.info.hard_words), np.uint32) if want_hard else None
         iters = np.empty(n, np.uint8) if want_iters else None
         tot = C.c_uint64()
-        fn = lib.ldpc_decode_int8_host if llr.dtype == np.int8 else lib.ldpc_decode_f32_host
-        if llr.dtype not in (np.int8, np.float32):
+        fns = {np.dtype(np.int8): lib.ldpc_decode_int8_host, np.dtype(np.float32): lib.ldpc_decode_f32_host,
+               np.dtype(np.int16): lib.ldpc_decode_int16_host, np.dtype(np.int32): lib.ldpc_decode_int32_host}
+        if llr.dtype not in fns:
             raise TypeError(llr.dtype)
+        fn = fns[llr.dtype]
         check(fn(self.h, llr.ctypes.data, n, _ptr(post), _ptr(hard), _ptr(iters), C.byref(tot)))
         return post, hard, iters, tot.value
 
