@@ -262,19 +262,20 @@ int ldpc_learned_decode(ldpc_ctx *ctx, const float *llr, size_t n, int iters, co
  * so every SNR point sees the same data and the same noise, scaled by its
  * sigma, as the reference's inner loop does (LDPCtop.cpp:89-97).
  * Outputs (dev):
- *   llr_i8 or llr_f32  [n_snr][n_per_snr][N]   (one of them, by variant)
+ *   llr_int or llr_f32 [n_snr][n_per_snr][N]   (one of them, by variant: llr_int
+ *                      holds int8, int16 or int32 elements, the context's type)
  *   data_bits          [n_per_snr][hard_words] sent data bits (optional)
  *   uncoded_err        [n_snr] sign errors before decoding (optional,
  *                      accumulated: caller zeroes)                         */
 int ldpc_generate(ldpc_ctx *ctx, uint64_t seed, uint64_t cw_offset, const float *snr_db, size_t n_snr,
-                  size_t n_per_snr, int8_t *llr_i8, float *llr_f32, uint32_t *data_bits,
+                  size_t n_per_snr, void *llr_int, float *llr_f32, uint32_t *data_bits,
                   unsigned long long *uncoded_err, void *stream);
 
 /* LLR quantisation of given noise (dev): cw_bits [n][N] 0/1 bytes,
  * noise [n][N] float -> llr [n][N] (int8 or float by variant) at one SNR.
  * Bit-exact restatement of gen_metrics(); used for parity checks. */
 int ldpc_llr_from_noise(ldpc_ctx *ctx, const uint8_t *cw_bits, const float *noise, size_t n, float snr_db,
-                        int8_t *llr_i8, float *llr_f32, unsigned long long *uncoded_err, void *stream);
+                        void *llr_int, float *llr_f32, unsigned long long *uncoded_err, void *stream);
 
 /* QC encoding (dev): data_bits [n][hard_words] packed -> cw_bits [n][N]
  * 0/1 bytes.  Replaces LDPCencode() (LDPCencode.cpp:40-100). */

@@ -79,11 +79,9 @@ void release_gen(ldpc_ctx* x) {
 }
 
 int launch_gen(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* snr_db, size_t n_snr, size_t n_per_snr,
-               int8_t* llr_i8, float* llr_f32, uint32_t* data_bits, unsigned long long* uncoded, cudaStream_t s) {
+               void* llr_int, float* llr_f32, uint32_t* data_bits, unsigned long long* uncoded, cudaStream_t s) {
     if (!x->code.has_enc) return fail(LDPC_ERR_INVALID_ARG, "code has no encoder table");
     if (!x->gen_ok) return fail(LDPC_ERR_UNSUPPORTED, "generator: %s", x->gen_err.c_str());
-    if (x->cfg.variant == LDPC_INT16_OMS || x->cfg.variant == LDPC_INT32_OMS)
-        return fail(LDPC_ERR_UNSUPPORTED, "generator: int16/int32 LLRs are not produced on the device");
     if (n_snr < 1 || n_snr > (size_t)GEN_MAX_SNR) return fail(LDPC_ERR_INVALID_ARG, "n_snr=%zu outside 1..%d", n_snr, GEN_MAX_SNR);
     if (!snr_db) return fail(LDPC_ERR_INVALID_ARG, "snr_db is NULL");
     if (n_per_snr == 0) return LDPC_OK;
@@ -95,7 +93,10 @@ int launch_gen(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* snr_
     job.n_snr = (int)n_snr;
     for (size_t i = 0; i < n_snr; ++i) sigma_of(snr_db[i], x->cfg.llr_scale, &job.sigma[i], &job.sigma_factor[i]);
     job.max_abs = x->cfg.max_abs_llr;
-    job.llr_i8 = llr_i8;
+    // integer LLRs of the context's element type
+    if (x->cfg.variant == LDPC_INT16_OMS) job.llr_i16 = (int16_t*)llr_int;
+    else if (x->cfg.variant == LDPC_INT32_OMS) job.llr_i32 = (int32_t*)llr_int;
+    else job.llr_i8 = (int8_t*)llr_int;
     job.llr_f32 = llr_f32;
     job.data_bits = data_bits;
     job.uncoded = uncoded;
@@ -113,10 +114,10 @@ using ldpc::fail;
 extern "C" {
 
 int ldpc_generate(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* snr_db, size_t n_snr, size_t n_per_snr,
-                  int8_t* llr_i8, float* llr_f32, uint32_t* data_bits, unsigned long long* uncoded, void* stream) {
+                  void* llr_int, float* llr_f32, uint32_t* data_bits, unsigned long long* uncoded, void* stream) {
     if (!x) return fail(LDPC_ERR_INVALID_ARG, "ctx is NULL");
     CUDA_TRY(cudaSetDevice(x->device));
-    return ldpc::launch_gen(x, seed, cw_offset, snr_db, n_snr, n_per_snr, llr_i8, llr_f32, data_bits, uncoded,
+    return ldpc::launch_gen(x, seed, cw_offset, snr_db, n_snr, n_per_snr, llr_int, llr_f32, data_bits, uncoded,
                             (cudaStream_t)stream);
 }
 
@@ -134,20 +135,22 @@ int ldpc_encode(ldpc_ctx* x, const uint32_t* data_bits, size_t n, uint8_t* cw_bi
     return LDPC_OK;
 }
 
-int ldpc_llr_from_noise(ldpc_ctx* x, const uint8_t* cw_bits, const float* noise, size_t n, float snr_db, int8_t* llr_i8,
+int ldpc_llr_from_noise(ldpc_ctx* x, const uint8_t* cw_bits, const float* noise, size_t n, float snr_db, void* llr_int,
                         float* llr_f32, unsigned long long* uncoded, void* stream) {
     if (!x) return fail(LDPC_ERR_INVALID_ARG, "ctx is NULL");
     if (!x->code.has_enc) return fail(LDPC_ERR_INVALID_ARG, "code has no encoder table (puncture/filler masks)");
     if (!x->gen_ok) return fail(LDPC_ERR_UNSUPPORTED, "generator: %s", x->gen_err.c_str());
     if (n == 0) return LDPC_OK;
-    if (!cw_bits || !noise || (!llr_i8 && !llr_f32)) return fail(LDPC_ERR_INVALID_ARG, "NULL buffer");
+    if (!cw_bits || !noise || (!llr_int && !llr_f32)) return fail(LDPC_ERR_INVALID_ARG, "NULL buffer");
+    const bool is_float = x->cfg.variant == LDPC_F32_SP || x->cfg.variant == LDPC_F32_OMS;
     CUDA_TRY(cudaSetDevice(x->device));
     float sigma, sf;
     ldpc::sigma_of(snr_db, x->cfg.llr_scale, &sigma, &sf);
     const long long total = (long long)n * x->n;
     const int grid = (int)std::min<long long>((total + 255) / 256, (long long)x->sms * 16);
     ldpc::llr_from_noise_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(x->gent, cw_bits, noise, total, sigma, sf,
-                                                                       x->cfg.max_abs_llr, llr_i8, llr_f32, uncoded);
+                                                                       x->cfg.max_abs_llr, is_float ? nullptr : llr_int,
+                                                                       ldpc::llr_bytes(x->cfg.variant), llr_f32, uncoded);
     CUDA_TRY(cudaGetLastError());
     return LDPC_OK;
 }
@@ -171,8 +174,8 @@ int ldpc_simulate(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* s
     if (!x || !snr_db || !stats) return fail(LDPC_ERR_INVALID_ARG, "NULL argument");
     if (n_snr < 1 || n_snr > (size_t)ldpc::GEN_MAX_SNR) return fail(LDPC_ERR_INVALID_ARG, "n_snr=%zu", n_snr);
     CUDA_TRY(cudaSetDevice(x->device));
-    const bool is8 = x->cfg.variant == LDPC_INT8_OMS;
-    const size_t N = (size_t)x->n, es = is8 ? 1 : 4;
+    const bool is_float = x->cfg.variant == LDPC_F32_SP || x->cfg.variant == LDPC_F32_OMS;
+    const size_t N = (size_t)x->n, es = (size_t)ldpc::llr_bytes(x->cfg.variant);
     // chunk so that the LLRs of all SNR points fit in ~2 GB
     size_t chunk = std::max<size_t>(1, std::min<size_t>(n_per_snr, ((size_t)2 << 30) / (n_snr * N * es)));
     if (x->sim_cap < chunk * n_snr) {
@@ -191,8 +194,8 @@ int ldpc_simulate(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* s
     std::vector<double> ms(n_snr, 0.0);
     for (size_t off = 0; off < n_per_snr; off += chunk) {
         const size_t m = std::min(chunk, n_per_snr - off);
-        int rc = ldpc::launch_gen(x, seed, cw_offset + off, snr_db, n_snr, m, is8 ? (int8_t*)x->d_sim_llr : nullptr,
-                                  is8 ? nullptr : (float*)x->d_sim_llr, (uint32_t*)x->d_sim_data,
+        int rc = ldpc::launch_gen(x, seed, cw_offset + off, snr_db, n_snr, m, is_float ? nullptr : x->d_sim_llr,
+                                  is_float ? (float*)x->d_sim_llr : nullptr, (uint32_t*)x->d_sim_data,
                                   dc + ldpc::OMS_MAX_BUCKETS * 4, s);
         if (rc) return rc;
         for (size_t k = 0; k < n_snr; ++k) {

@@ -223,6 +223,13 @@ __global__ void __launch_bounds__(256) gen_kernel(const __grid_constant__ GenTab
                         for (int q = 0; q < 4 && idx0 + q < tb.n; ++q) dst[q] = (int8_t)(packed >> (8 * q));
                     }
                 }
+                if (job.llr_i16 || job.llr_i32) {
+                    for (int q = 0; q < 4 && idx0 + q < tb.n; ++q) {
+                        const int v = __float2int_rn(l[q]);           // roundi (nearest-even)
+                        if (job.llr_i16) job.llr_i16[row * tb.n + idx0 + q] = (int16_t)v;   // compress: wrap to 16 bits
+                        if (job.llr_i32) job.llr_i32[row * tb.n + idx0 + q] = v;
+                    }
+                }
                 if (job.llr_f32) {
                     float* dst = job.llr_f32 + row * tb.n + idx0;
                     if ((tb.n & 3) == 0) {
@@ -275,7 +282,7 @@ __global__ void __launch_bounds__(256) encode_kernel(const __grid_constant__ Gen
 
 // gen_metrics on given noise: elementwise.
 __global__ void llr_from_noise_kernel(const GenTables tb, const uint8_t* bits, const float* noise, long long total,
-                                      float sigma, float sf, float max_abs, int8_t* out_i8, float* out_f32,
+                                      float sigma, float sf, float max_abs, void* out_int, int int_bytes, float* out_f32,
                                       unsigned long long* uncoded) {
     unsigned long long err = 0;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
@@ -283,7 +290,11 @@ __global__ void llr_from_noise_kernel(const GenTables tb, const uint8_t* bits, c
         float l;
         err += llr_element(bits[e] & 1, noise[e], sigma, sf, max_abs, tb.any_punct ? tb.punct[idx] : 0,
                            tb.any_filler ? tb.filler[idx] : 0, &l);
-        if (out_i8) out_i8[e] = llr_to_i8(l);
+        if (out_int) {
+            if (int_bytes == 1) static_cast<int8_t*>(out_int)[e] = llr_to_i8(l);
+            else if (int_bytes == 2) static_cast<int16_t*>(out_int)[e] = (int16_t)__float2int_rn(l);
+            else static_cast<int32_t*>(out_int)[e] = __float2int_rn(l);
+        }
         if (out_f32) out_f32[e] = l;
     }
     if (uncoded) {

@@ -163,7 +163,7 @@ int setup_sp(ldpc_ctx* x);
 int launch_sp(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s);
 int setup_gen(ldpc_ctx* x);
 int launch_gen(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* snr_db, size_t n_snr, size_t n_per_snr,
-               int8_t* llr_i8, float* llr_f32, uint32_t* data_bits, unsigned long long* uncoded, cudaStream_t s);
+               void* llr_int, float* llr_f32, uint32_t* data_bits, unsigned long long* uncoded, cudaStream_t s);
 void release_gen(ldpc_ctx* x);
 uint32_t half2_bits(float v);
 int8_t max_row_i8(float max_row_metric);   // decode_row's Max_row_simd, int8 build

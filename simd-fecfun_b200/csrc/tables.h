@@ -152,6 +152,8 @@ struct GenJob {
     float sigma_factor[GEN_MAX_SNR];
     float max_abs;
     int8_t* llr_i8;                  // [n_snr][n_per_snr][n] or null
+    int16_t* llr_i16;                // int16 contexts (gen_metrics: roundi, then compress)
+    int32_t* llr_i32;                // int32 contexts (gen_metrics: roundi)
     float* llr_f32;                  // [n_snr][n_per_snr][n] or null
     uint32_t* data_bits;             // [n_per_snr][hard_words] or null
     unsigned long long* uncoded;     // [n_snr] or null

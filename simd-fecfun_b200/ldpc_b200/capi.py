@@ -233,12 +233,16 @@ class Context:
                                     bucket_size, _ptr(counters), n_buckets, stream or None))
 
     def generate(self, seed, cw_offset, snr_db, n_per_snr, llr_i8=None, llr_f32=None, data_bits=None, uncoded=None,
-                 stream=0):
+                 stream=0, llr_int=None):
+        """llr_int (alias llr_i8): integer LLRs of the context's element type."""
+        llr_i8 = llr_int if llr_int is not None else llr_i8
         snr = np.ascontiguousarray(snr_db, dtype=np.float32)
         check(lib.ldpc_generate(self.h, seed, cw_offset, snr.ctypes.data, snr.size, n_per_snr, _ptr(llr_i8),
                                 _ptr(llr_f32), _ptr(data_bits), _ptr(uncoded), stream or None))
 
-    def llr_from_noise(self, cw_bits, noise, n, snr_db, llr_i8=None, llr_f32=None, uncoded=None, stream=0):
+    def llr_from_noise(self, cw_bits, noise, n, snr_db, llr_i8=None, llr_f32=None, uncoded=None, stream=0,
+                       llr_int=None):
+        llr_i8 = llr_int if llr_int is not None else llr_i8
         check(lib.ldpc_llr_from_noise(self.h, _ptr(cw_bits), _ptr(noise), n, snr_db, _ptr(llr_i8), _ptr(llr_f32),
                                       _ptr(uncoded), stream or None))
 

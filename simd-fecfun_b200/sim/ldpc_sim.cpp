@@ -14,8 +14,8 @@
 //           (LDPCtop.cpp:127-129), which run_LDPCsim.pl:159-178 parses.
 //
 // The decoder variant comes from the program name, as the Perl driver reads
-// it (run_LDPCsim.pl:51-66): "_prod" -> float sum-product, "f_min" -> float
-// offset min-sum, otherwise int8 offset min-sum.
+// it (run_LDPCsim.pl:51-66): Vec<n>c / s / w -> int8 / int16 / int32 offset
+// min-sum, Vec<n>f -> float offset min-sum, or sum-product with "_prod".
 //
 // Differences from the reference, by design:
 //   - noise and data come from Philox4x32-10 keyed by one 64-bit value that
@@ -34,6 +34,7 @@
 #include <cinttypes>
 #include <cstdio>
 #include <cstdlib>
+#include <cctype>
 #include <cstring>
 #include <random>
 #include <string>
@@ -85,11 +86,25 @@ double tsc_per_second() {
     exit(1);
 }
 
+// run_LDPCsim.pl:51-66 reads "Vec<lanes><type>" from the program name
+// (c int8, s int16, w int32, f float, d double) and "_prod" for sum-product.
 int variant_from_name(const char* argv0) {
     const std::string name = argv0 ? argv0 : "";
-    if (name.find("_prod") != std::string::npos) return LDPC_F32_SP;
-    if (name.find("f_min") != std::string::npos) return LDPC_F32_OMS;
-    return LDPC_INT8_OMS;
+    const size_t v = name.rfind("Vec");
+    char type = 'c';
+    if (v != std::string::npos) {
+        size_t i = v + 3;
+        while (i < name.size() && isdigit((unsigned char)name[i])) ++i;
+        if (i < name.size() && i > v + 3) type = name[i];
+    }
+    const bool prod = name.find("_prod") != std::string::npos;
+    switch (type) {
+        case 's': return LDPC_INT16_OMS;
+        case 'w': return LDPC_INT32_OMS;
+        case 'f': return prod ? LDPC_F32_SP : LDPC_F32_OMS;
+        case 'd': return -1;
+        default: return prod ? -1 : LDPC_INT8_OMS;
+    }
 }
 
 }  // namespace
@@ -122,6 +137,10 @@ int main(int argc, char** argv) {
 
     ldpc_cfg cfg;
     cfg.variant = variant_from_name(argv[0]);
+    if (cfg.variant < 0) {
+        printf("ERROR: decoder variant of %s is not built (double, or sum-product on integers)\n", argv[0]);
+        return 1;
+    }
     cfg.max_iter = sim.max_iter;
     cfg.max_row_metric = sim.max_row_metric;
     cfg.beta = sim.beta_offset;

@@ -132,3 +132,42 @@ def test_generate_consistency_and_noise_statistics(capi, oracle):
     ctx.generate(123, 1000 + 7, snrs[:1], 16, llr_f32=llr[0], data_bits=data2)
     torch.cuda.synchronize()
     assert np.array_equal(data2.cpu().numpy()[:9], data.cpu().numpy()[7:16])
+
+
+@pytest.mark.parametrize("variant,bits,scale,max_abs", [("Vec32s_min", 16, 40.0, 1000.0), ("Vec16w_min", 32, 4000.0, 1e6)])
+def test_integer_llrs_match_reference_gen_metrics(capi, variant, bits, scale, max_abs):
+    """int16 / int32 LLRs (roundi, then compress for int16) against the
+    reference's gen_metrics of the matching build, on the same noise."""
+    import torch
+    import refbind as rb
+    from ldpc_b200 import codes
+    if not rb.ref_available(variant):
+        pytest.skip("reference build absent")
+    lib = rb.RefLib(variant)
+    code = codes.make_code("11ad 1/2", elem_size=bits)
+    n = 48
+    ref = rb.RefCtx(lib, code, n)
+    rng = np.random.default_rng(2)
+    ref.set_info_bits(rng.integers(0, 2, (n, code.z * 8), dtype=np.uint8))
+    ref.encode()
+    cw = ref.codeword_bits()
+    zb = (code.z + 7) // 8 * 8
+    wgn = np.zeros((n, code.mcol, zb), np.float32)
+    wgn[:, :, :code.z] = rng.standard_normal((n, code.mcol, code.z), dtype=np.float32)
+    flat = np.zeros(ref.wgn_count() * 8, np.float32)
+    flat[:wgn.size] = wgn.ravel()
+    unc_ref = ref.gen_metrics(0.25, flat, scale, max_abs)
+    llr_ref = ref.posteriors()
+    ctx = capi.Context(capi.Code.from_tables(code), variant=capi.LDPC_INT16_OMS if bits == 16 else capi.LDPC_INT32_OMS,
+                       llr_scale=scale, max_abs_llr=max_abs)
+    dt = torch.int16 if bits == 16 else torch.int32
+    out = torch.empty((n, code.n), dtype=dt, device="cuda")
+    unc = torch.zeros(1, dtype=torch.int64, device="cuda")
+    noise = np.ascontiguousarray(wgn[:, :, :code.z].reshape(n, code.n))
+    ctx.llr_from_noise(torch.from_numpy(cw).cuda(), torch.from_numpy(noise).cuda(), n, 0.25, llr_int=out, uncoded=unc)
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), llr_ref)
+    assert int(unc.item()) == unc_ref
+    # the fused generator quantises the same way: its int16/int32 LLRs decode in simulate
+    st = ctx.simulate(seed=5, cw_offset=0, snr_db=[1.0], n_per_snr=5000)[0]
+    assert st["codewords"] == 5000 and st["iterations"] >= 5000
