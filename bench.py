@@ -234,7 +234,7 @@ def run_workload(args):
     elif args.workload == "hetero-mix":
         out = workloads.hetero_mix(steps=args.steps, warmup=args.warmup)
     elif args.workload == "sp-sweep":
-        out = workloads.sp_sweep(cw_per_z=args.sp_cw)
+        out = workloads.sp_sweep(cw_per_z=args.sp_cw, steps=args.steps, warmup=args.warmup)
     else:
         out = workloads.learned_run(train_steps=max(args.steps, 2), batch=args.learned_batch)
     out["clocks"] = _clock_summary(clk)

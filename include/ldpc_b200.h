@@ -168,8 +168,9 @@ int ldpc_decode_set_compat(ldpc_ctx *ctx, void *decoded_metrics, unsigned num_co
  * No counterpart in the reference: it runs one code per process
  * (build/run_LDPCsim.pl:102-109) and one codeword at a time
  * (LDPCdecode.cpp:227-243).  A batch holds several codes, each with its own
- * configuration (int8 offset min-sum only) and optionally one int8 offset
- * per layer (learned offsets).  A plan fixes a list of jobs (device buffers
+ * configuration; all codes use the same variant (LDPC_INT8_OMS, LDPC_F32_SP or
+ * LDPC_F32_OMS).  int8 batches also take one int8 offset per layer (learned
+ * offsets).  A plan fixes a list of jobs (device buffers
  * of one code each) and splits them into chunks of equal work.  A plan's
  * launch is ONE persistent kernel over all jobs, and it can be replayed
  * from a CUDA graph.  Per codeword, the results are exactly those of
@@ -179,9 +180,9 @@ typedef struct ldpc_batch_plan ldpc_batch_plan;
 
 typedef struct {
     int code;                       /* index of the code in the batch */
-    const int8_t *llr;              /* dev [n][N_code] */
+    const void *llr;                /* dev [n][N_code], int8 or float by the batch's variant */
     size_t n;
-    int8_t *post_out;               /* dev, optional (NULL) */
+    void *post_out;                 /* dev, optional (NULL); element type as llr */
     uint32_t *hard_out;             /* dev [n][hard_words], optional */
     uint8_t *iters_out;             /* dev [n], optional */
     const uint32_t *data_bits;      /* dev, optional: fused counting as ldpc_decode_count */

@@ -8,11 +8,14 @@
 #include <vector>
 
 #include "internal.h"
+#include "sp_batch.cuh"
 
 using ldpc::fail;
 
 struct ldpc_batch {
     int device = 0, sms = 0;
+    int variant = LDPC_INT8_OMS;             // every code of a batch runs the same decoder
+    std::vector<float> maxf;                 // float batches: decode_row's Max_val per code
     std::vector<ldpc_code> codes;
     std::vector<ldpc_cfg> cfgs;
     std::vector<std::vector<int>> beta8;     // per code, per layer
@@ -22,13 +25,16 @@ struct ldpc_batch {
 
 struct ldpc_batch_plan {
     int device = 0;
-    ldpc::RtLaunch lp;
+    bool is_float = false;
+    ldpc::RtLaunch lp;                       // int8 batches
     ldpc::rt_fn k = nullptr;
-    int threads = 0, smem = 0, grid = 0;
-    ldpc::RtCode* d_codes = nullptr;
-    ldpc::RtJob* d_jobs = nullptr;
+    ldpc::SpBatchLaunch slp;                 // float batches
+    void* kf = nullptr;
+    int threads = 0, smem = 0, grid = 0, n_chunks = 0;
+    void* d_codes = nullptr;
+    void* d_jobs = nullptr;
     ldpc::RtChunk* d_chunks = nullptr;
-    uint32_t* d_scratch = nullptr;
+    void* d_scratch = nullptr;
     cudaStream_t own = nullptr;              // graph capture and replay stream
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     cudaGraph_t graph = nullptr;
@@ -39,15 +45,32 @@ namespace {
 
 constexpr int kTunedWidths[] = {128, 192, 256, 320, 384, 448, 512};
 
+typedef void (*spb_fn)(const ldpc::SpBatchLaunch);
+struct SpbVariant {
+    int dmax;
+    bool prod, rsmem;
+    spb_fn k;
+};
+#define SPB(D_, P_, R_) {D_, P_, R_, ldpc::sp_batch_kernel<D_, P_, R_>}
+const SpbVariant kSpb[] = {SPB(8, true, true),   SPB(8, true, false),   SPB(8, false, true),   SPB(8, false, false),
+                           SPB(16, true, true),  SPB(16, true, false),  SPB(16, false, true),  SPB(16, false, false),
+                           SPB(32, true, true),  SPB(32, true, false),  SPB(32, false, true),  SPB(32, false, false)};
+#undef SPB
+
+void launch_plan_kernel(ldpc_batch_plan* p, cudaStream_t s) {
+    if (p->is_float) ((spb_fn)p->kf)<<<p->grid, p->threads, p->smem, s>>>(p->slp);
+    else p->k<<<p->grid, p->threads, p->smem, s>>>(p->lp);
+}
+
 // Chunks of about equal work (codewords x edges per codeword) so that the
 // strided chunk-to-CTA assignment balances the CTAs.
-void make_chunks(const std::vector<ldpc::RtJob>& jobs, const std::vector<long long>& cost_per_cw,
+void make_chunks(const std::vector<long long>& ncw, const std::vector<long long>& cost_per_cw,
                  const std::vector<int>& min_chunk, long long target_chunks, std::vector<ldpc::RtChunk>& out) {
     double total = 0;
-    for (size_t j = 0; j < jobs.size(); ++j) total += (double)jobs[j].ncw * (double)cost_per_cw[j];
+    for (size_t j = 0; j < ncw.size(); ++j) total += (double)ncw[j] * (double)cost_per_cw[j];
     const double per_chunk = std::max(1.0, total / (double)std::max(1LL, target_chunks));
-    for (size_t j = 0; j < jobs.size(); ++j) {
-        const long long n = jobs[j].ncw;
+    for (size_t j = 0; j < ncw.size(); ++j) {
+        const long long n = ncw[j];
         if (n == 0) continue;
         long long m = (long long)std::llround((double)n * (double)cost_per_cw[j] / per_chunk);
         m = std::max(1LL, std::min(m, std::max(1LL, n / min_chunk[j])));
@@ -94,6 +117,109 @@ struct PlanDel {
     }
 };
 
+int float_plan(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int threads, int cpc, ldpc_batch_plan** out) {
+    const int nc = (int)b->codes.size();
+    const bool prod = b->variant == LDPC_F32_SP;
+    std::vector<int> G(nc, 1);
+    std::vector<size_t> base(nc);
+    int dmax = 8, maxE = 0;
+    bool rsmem = true;
+    for (int c = 0; c < nc; ++c) {
+        const ldpc_code& cd = b->codes[c];
+        const int n = cd.z * cd.mcol, E = (int)cd.row_cols.size();
+        auto bytes = [&](int g) {
+            ldpc::SpTables t;
+            ldpc::fill_sp_tables(cd, g, &t);
+            return (size_t)ldpc::sp_code_bytes() + (((size_t)g * t.stride + 3) & ~(size_t)3) * 4 + (size_t)g * ((n + 3) & ~3) * 4;
+        };
+        G[c] = std::max(1, std::min(32, threads / cd.z));
+        while (G[c] > 1 && bytes(G[c]) > (size_t)ldpc::kSpMaxSmem) --G[c];
+        base[c] = bytes(G[c]);
+        if (base[c] > (size_t)ldpc::kSpMaxSmem)
+            return fail(LDPC_ERR_UNSUPPORTED, "batch plan: code %d (N=%d) does not fit shared memory", c, n);
+        if (base[c] + (size_t)E * threads * 4 > (size_t)ldpc::kSpMaxSmem) rsmem = false;
+        dmax = std::max(dmax, cd.max_row_weight <= 8 ? 8 : cd.max_row_weight <= 16 ? 16 : 32);
+        maxE = std::max(maxE, E);
+    }
+    size_t smem = 0;
+    for (int c = 0; c < nc; ++c) smem = std::max(smem, base[c] + (rsmem ? (size_t)b->codes[c].row_cols.size() * threads * 4 : 0));
+    spb_fn k = nullptr;
+    for (const SpbVariant& v : kSpb)
+        if (v.dmax == dmax && v.prod == prod && v.rsmem == rsmem) k = v.k;
+    std::unique_ptr<ldpc_batch_plan, PlanDel> p(new ldpc_batch_plan);
+    p->device = b->device;
+    p->is_float = true;
+    p->kf = (void*)k;
+    p->threads = threads;
+    p->smem = (int)smem;
+    CUDA_TRY(ldpc::allow_dynamic_smem((const void*)k, ldpc::kSpMaxSmem));
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k, threads, smem));
+    if (per_sm < 1) return fail(LDPC_ERR_UNSUPPORTED, "batch plan: %d threads x %zu B do not fit an SM", threads, smem);
+    const long long ctas = (long long)per_sm * b->sms;
+    std::vector<ldpc::SpCode> hc(nc);
+    for (int c = 0; c < nc; ++c) {
+        memset(&hc[c], 0, sizeof(hc[c]));
+        ldpc::fill_sp_tables(b->codes[c], G[c], &hc[c].t);
+        hc[c].max_iter = (int)b->cfgs[c].max_iter;
+        hc[c].num_par = b->codes[c].num_par;
+        hc[c].beta = b->cfgs[c].beta;
+        hc[c].maxv = b->maxf[c];
+    }
+    std::vector<ldpc::SpBatchJob> hj(n_jobs);
+    std::vector<long long> ncw(n_jobs), cost(n_jobs);
+    std::vector<int> minc(n_jobs);
+    for (int i = 0; i < n_jobs; ++i) {
+        const ldpc_batch_job& s = jobs[i];
+        ldpc::SpBatchJob& j = hj[i];
+        memset(&j, 0, sizeof(j));
+        j.llr = (const float*)s.llr;
+        j.ncw = (long long)s.n;
+        j.post_out = (float*)s.post_out;
+        j.hard_out = s.hard_out;
+        j.iters_out = s.iters_out;
+        j.ref_bits = s.data_bits;
+        j.ref_period = s.ref_period > 0 ? (long long)s.ref_period : 1;
+        j.bucket_size = s.bucket_size > 0 ? (long long)s.bucket_size : std::max(1LL, (long long)s.n);
+        j.counters = s.counters;
+        j.n_buckets = std::max(1, std::min(s.n_buckets, ldpc::OMS_MAX_BUCKETS));
+        j.code = s.code;
+        const ldpc_code& cd = b->codes[s.code];
+        ncw[i] = j.ncw;
+        cost[i] = (long long)cd.row_cols.size() * cd.z;
+        minc[i] = 4 * G[s.code];
+    }
+    std::vector<ldpc::RtChunk> chunks;
+    make_chunks(ncw, cost, minc, ctas * cpc, chunks);
+    const int n_chunks = (int)chunks.size();
+    p->grid = (int)std::max(1LL, std::min<long long>(ctas, n_chunks));
+    CUDA_TRY(cudaMalloc(&p->d_codes, sizeof(ldpc::SpCode) * nc));
+    CUDA_TRY(cudaMemcpy(p->d_codes, hc.data(), sizeof(ldpc::SpCode) * nc, cudaMemcpyHostToDevice));
+    if (n_jobs) {
+        CUDA_TRY(cudaMalloc(&p->d_jobs, sizeof(ldpc::SpBatchJob) * n_jobs));
+        CUDA_TRY(cudaMemcpy(p->d_jobs, hj.data(), sizeof(ldpc::SpBatchJob) * n_jobs, cudaMemcpyHostToDevice));
+    }
+    if (n_chunks) {
+        CUDA_TRY(cudaMalloc(&p->d_chunks, sizeof(ldpc::RtChunk) * n_chunks));
+        CUDA_TRY(cudaMemcpy(p->d_chunks, chunks.data(), sizeof(ldpc::RtChunk) * n_chunks, cudaMemcpyHostToDevice));
+    }
+    long long words = 0;
+    if (!rsmem) {
+        words = (long long)maxE * threads;
+        CUDA_TRY(cudaMalloc(&p->d_scratch, (size_t)p->grid * words * 4));
+    }
+    memset(&p->slp, 0, sizeof(p->slp));
+    p->slp.codes = (const ldpc::SpCode*)p->d_codes;
+    p->slp.jobs = (const ldpc::SpBatchJob*)p->d_jobs;
+    p->slp.chunks = p->d_chunks;
+    p->slp.n_chunks = p->d_jobs ? n_chunks : 0;
+    p->slp.r_scratch = (float*)p->d_scratch;
+    p->slp.r_words_per_cta = words;
+    p->n_chunks = p->slp.n_chunks;
+    *out = p.release();
+    return LDPC_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -115,8 +241,21 @@ int ldpc_batch_create(const ldpc_code* const* codes, const ldpc_cfg* cfgs, int n
         if (!codes[i]) return fail(LDPC_ERR_INVALID_ARG, "batch: code %d is NULL", i);
         const ldpc_code& c = *codes[i];
         const ldpc_cfg& g = cfgs[i];
-        if (g.variant != LDPC_INT8_OMS) return fail(LDPC_ERR_UNSUPPORTED, "batch: code %d: only the int8 decoder is batched", i);
+        if (i == 0) b->variant = g.variant;
+        if (g.variant != b->variant)
+            return fail(LDPC_ERR_UNSUPPORTED, "batch: code %d: every code of a batch needs the same variant", i);
         if (g.max_iter < 1 || g.max_iter > 255) return fail(LDPC_ERR_UNSUPPORTED, "batch: code %d: max_iter=%u", i, g.max_iter);
+        if (g.variant == LDPC_F32_SP || g.variant == LDPC_F32_OMS) {
+            if (c.mrow > ldpc::SP_MAX_L || (int)c.row_cols.size() > ldpc::SP_MAX_E || c.max_row_weight > 32 || c.z > 512)
+                return fail(LDPC_ERR_UNSUPPORTED, "batch: code %d exceeds the float decoder's tables", i);
+            b->codes.push_back(c);
+            b->cfgs.push_back(g);
+            b->beta8.push_back(std::vector<int>(c.mrow, 0));
+            b->maxv2.push_back(0);
+            b->maxf.push_back(g.max_row_metric < 1e-6f ? (float)(1.0 - (double)g.max_row_metric) : g.max_row_metric);
+            continue;
+        }
+        if (g.variant != LDPC_INT8_OMS) return fail(LDPC_ERR_UNSUPPORTED, "batch: code %d: variant %d is not batched", i, g.variant);
         if (!(g.beta >= 0.0f && g.beta < 128.0f)) return fail(LDPC_ERR_UNSUPPORTED, "batch: code %d: beta=%g", i, g.beta);
         if (!(g.max_row_metric > -128.0f && g.max_row_metric < 128.0f))
             return fail(LDPC_ERR_UNSUPPORTED, "batch: code %d: max_row_metric=%g", i, g.max_row_metric);
@@ -130,6 +269,7 @@ int ldpc_batch_create(const ldpc_code* const* codes, const ldpc_cfg* cfgs, int n
         b->cfgs.push_back(g);
         b->beta8.push_back(std::vector<int>(c.mrow, (int)(int8_t)g.beta));
         b->maxv2.push_back(ldpc::half2_bits((float)max8));
+        b->maxf.push_back(0.f);
     }
     *out = b.release();
     return LDPC_OK;
@@ -137,6 +277,7 @@ int ldpc_batch_create(const ldpc_code* const* codes, const ldpc_cfg* cfgs, int n
 
 int ldpc_batch_set_offsets(ldpc_batch* b, int code, const float* beta) {
     if (!b) return fail(LDPC_ERR_INVALID_ARG, "batch is NULL");
+    if (b->variant != LDPC_INT8_OMS) return fail(LDPC_ERR_UNSUPPORTED, "per-layer offsets are for int8 batches");
     if (code < 0 || code >= (int)b->codes.size()) return fail(LDPC_ERR_INVALID_ARG, "code %d of %zu", code, b->codes.size());
     std::vector<int>& v = b->beta8[code];
     for (size_t l = 0; l < v.size(); ++l) {
@@ -166,6 +307,7 @@ int ldpc_batch_plan_create(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs
     if (threads % 32 || threads > ldpc::kRtMaxThreads || threads < maxz)
         return fail(LDPC_ERR_UNSUPPORTED, "batch plan: %d threads per CTA (multiple of 32, >= Z=%d, <= %d)", threads, maxz,
                     ldpc::kRtMaxThreads);
+    if (b->variant != LDPC_INT8_OMS) return float_plan(b, jobs, n_jobs, threads, cpc, out);
     std::vector<int> G(nc, 1);
     int dmax = 8, maxE = 0;
     bool quirk = false, rsmem = true;
@@ -210,9 +352,9 @@ int ldpc_batch_plan_create(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs
         const ldpc_batch_job& s = jobs[i];
         ldpc::RtJob& j = hj[i];
         memset(&j, 0, sizeof(j));
-        j.llr = s.llr;
+        j.llr = (const int8_t*)s.llr;
         j.ncw = (long long)s.n;
-        j.post_out = s.post_out;
+        j.post_out = (int8_t*)s.post_out;
         j.hard_out = s.hard_out;
         j.iters_out = s.iters_out;
         j.ref_bits = s.data_bits;
@@ -226,7 +368,9 @@ int ldpc_batch_plan_create(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs
         minc[i] = 8 * G[s.code];     // a chunk keeps its 2G slots busy for a while
     }
     std::vector<ldpc::RtChunk> chunks;
-    make_chunks(hj, cost, minc, ctas * cpc, chunks);
+    std::vector<long long> ncw(n_jobs);
+    for (int i = 0; i < n_jobs; ++i) ncw[i] = hj[i].ncw;
+    make_chunks(ncw, cost, minc, ctas * cpc, chunks);
     const int n_chunks = (int)chunks.size();
     p->grid = (int)std::max(1LL, std::min<long long>(ctas, n_chunks));
     CUDA_TRY(cudaMalloc(&p->d_codes, sizeof(ldpc::RtCode) * nc));
@@ -245,36 +389,37 @@ int ldpc_batch_plan_create(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs
         CUDA_TRY(cudaMalloc(&p->d_scratch, (size_t)p->grid * words * 4));
     }
     memset(&p->lp, 0, sizeof(p->lp));
-    p->lp.codes = p->d_codes;
-    p->lp.jobs = p->d_jobs;
+    p->lp.codes = (const ldpc::RtCode*)p->d_codes;
+    p->lp.jobs = (const ldpc::RtJob*)p->d_jobs;
     p->lp.chunks = p->d_chunks;
     p->lp.n_chunks = n_chunks;
-    p->lp.r_scratch = p->d_scratch;
+    p->lp.r_scratch = (uint32_t*)p->d_scratch;
     p->lp.r_words_per_cta = words;
     if (!p->d_jobs) p->lp.n_chunks = 0;
+    p->n_chunks = p->lp.n_chunks;
     *out = p.release();
     return LDPC_OK;
 }
 
 int ldpc_batch_plan_launch(ldpc_batch_plan* p, void* stream) {
     if (!p) return fail(LDPC_ERR_INVALID_ARG, "plan is NULL");
-    if (!p->lp.jobs || p->lp.n_chunks == 0) return LDPC_OK;
+    if (p->n_chunks == 0) return LDPC_OK;
     CUDA_TRY(cudaSetDevice(p->device));
-    p->k<<<p->grid, p->threads, p->smem, (cudaStream_t)stream>>>(p->lp);
+    launch_plan_kernel(p, (cudaStream_t)stream);
     CUDA_TRY(cudaGetLastError());
     return LDPC_OK;
 }
 
 int ldpc_batch_plan_graph_launch(ldpc_batch_plan* p, void* stream) {
     if (!p) return fail(LDPC_ERR_INVALID_ARG, "plan is NULL");
-    if (!p->lp.jobs || p->lp.n_chunks == 0) return LDPC_OK;
+    if (p->n_chunks == 0) return LDPC_OK;
     CUDA_TRY(cudaSetDevice(p->device));
     if (!p->exec) {
         CUDA_TRY(cudaStreamCreateWithFlags(&p->own, cudaStreamNonBlocking));
         CUDA_TRY(cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming));
         CUDA_TRY(cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming));
         CUDA_TRY(cudaStreamBeginCapture(p->own, cudaStreamCaptureModeThreadLocal));
-        p->k<<<p->grid, p->threads, p->smem, p->own>>>(p->lp);
+        launch_plan_kernel(p, p->own);
         const cudaError_t le = cudaGetLastError();
         cudaGraph_t g = nullptr;
         const cudaError_t ce = cudaStreamEndCapture(p->own, &g);

@@ -23,22 +23,15 @@ const SpVariant kSp[] = {
 #undef SPV
 }  // namespace
 
-int setup_sp(ldpc_ctx* x) {
-    const ldpc_code& c = x->code;
-    const bool prod = x->cfg.variant == LDPC_F32_SP;
-    if (c.mrow > SP_MAX_L || (int)c.row_cols.size() > SP_MAX_E)
-        return fail(LDPC_ERR_UNSUPPORTED, "float decoder: %d layers / %zu edges exceed the tables", c.mrow,
-                    c.row_cols.size());
-    const int dmax = c.max_row_weight <= 8 ? 8 : c.max_row_weight <= 16 ? 16 : c.max_row_weight <= 32 ? 32 : 0;
-    if (!dmax) return fail(LDPC_ERR_UNSUPPORTED, "float decoder: row weight %d > 32", c.max_row_weight);
-    SpTables& t = x->spt;
+void fill_sp_tables(const ldpc_code& c, int G, SpTables* out) {
+    SpTables& t = *out;
     memset(&t, 0, sizeof(t));
     t.z = c.z;
     t.mcol = c.mcol;
     t.n = c.z * c.mcol;
     t.L = c.mrow;
-    t.kbits = x->kbits;
-    t.hard_words = x->hard_words;
+    t.kbits = c.z * (c.mcol - c.mrow);
+    t.hard_words = (t.kbits + 31) / 32;
     t.E = (int)c.row_cols.size();
     int e0 = 0;
     for (int l = 0; l < c.mrow; ++l) {
@@ -50,12 +43,24 @@ int setup_sp(ldpc_ctx* x) {
         t.colz[e] = c.row_cols[e] * c.z;
         t.shift[e] = (int16_t)c.row_shifts[e];
     }
+    t.G = G;
+    t.stride = t.n + ((((32 + G - 1) / G) - t.n) % 32 + 32) % 32;
+}
+
+int setup_sp(ldpc_ctx* x) {
+    const ldpc_code& c = x->code;
+    const bool prod = x->cfg.variant == LDPC_F32_SP;
+    if (c.mrow > SP_MAX_L || (int)c.row_cols.size() > SP_MAX_E)
+        return fail(LDPC_ERR_UNSUPPORTED, "float decoder: %d layers / %zu edges exceed the tables", c.mrow,
+                    c.row_cols.size());
+    const int dmax = c.max_row_weight <= 8 ? 8 : c.max_row_weight <= 16 ? 16 : c.max_row_weight <= 32 ? 32 : 0;
+    if (!dmax) return fail(LDPC_ERR_UNSUPPORTED, "float decoder: row weight %d > 32", c.max_row_weight);
+    SpTables& t = x->spt;
     if (c.z > SP_MAXT) return fail(LDPC_ERR_UNSUPPORTED, "float decoder: Z=%d > %d", c.z, SP_MAXT);
     int G = std::max(1, std::min(32, 128 / c.z));
     if (const char* e = getenv("LDPC_SP_G")) G = std::max(1, std::min(32, atoi(e)));
     while (G > 1 && ((G * c.z + 31) / 32) * 32 > SP_MAXT) --G;
-    t.G = G;
-    t.stride = t.n + ((((32 + G - 1) / G) - t.n) % 32 + 32) % 32;
+    fill_sp_tables(c, G, &t);
     x->sp_threads = ((G * c.z + 31) / 32) * 32;
     const int nstage = (t.n + 3) & ~3;
     const size_t base_smem = ((((size_t)G * t.stride + 3) & ~(size_t)3) + (size_t)G * nstage) * 4;

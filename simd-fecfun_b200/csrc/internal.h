@@ -160,6 +160,8 @@ inline int llr_bytes(int variant) {
     return variant == LDPC_INT8_OMS ? 1 : variant == LDPC_INT16_OMS ? 2 : 4;
 }
 int setup_sp(ldpc_ctx* x);
+// float-decoder tables of a code for G codewords per CTA
+void fill_sp_tables(const ldpc_code& c, int G, SpTables* t);
 int launch_sp(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s);
 int setup_gen(ldpc_ctx* x);
 int launch_gen(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* snr_db, size_t n_snr, size_t n_per_snr,

@@ -47,9 +47,12 @@ __device__ __forceinline__ void sp_prefetch(float* stage, const float* llr, long
     }
 }
 
-template <int DMAX, bool PROD, bool RSMEM, int MAXT>
-__global__ void __launch_bounds__(MAXT) sp_f32_kernel(const __grid_constant__ SpTables tb, const __grid_constant__ SpJob job) {
-    extern __shared__ float sm_f[];
+// Decode codewords [lo, hi) of job with the CTA: the whole decoder; sm_f is
+// the CTA's dynamic shared memory for posteriors, staging and (RSMEM)
+// messages, r_cta its global message area otherwise.
+template <int DMAX, bool PROD, bool RSMEM>
+__device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJob& job, long long lo, long long hi,
+                                                float* sm_f, float* r_cta) {
     __shared__ long long s_cur[32];
     __shared__ long long s_next[32];
     __shared__ int s_it[32];
@@ -68,9 +71,8 @@ __global__ void __launch_bounds__(MAXT) sp_f32_kernel(const __grid_constant__ Sp
     float* Ps = sm_f;
     float* stage = sm_f + ((G * stride + 3) & ~3);                  // [G][nstage], 16-byte aligned
     const int nstage = (n + 3) & ~3;
-    float* Rbase = RSMEM ? stage + G * nstage : job.r_scratch + (long long)blockIdx.x * tb.E * nthr;
+    float* Rbase = RSMEM ? stage + G * nstage : r_cta;
     float* Rt = Rbase + tid;                                        // message of edge e at Rt[e * nthr]
-    const long long lo = job.ncw * blockIdx.x / gridDim.x, hi = job.ncw * (blockIdx.x + 1) / gridDim.x;
     const float beta = job.beta, maxv = job.maxv;
 
     for (int i = tid; i < OMS_MAX_BUCKETS * 4; i += nthr) (&s_cnt[0][0])[i] = 0;
@@ -237,6 +239,14 @@ __global__ void __launch_bounds__(MAXT) sp_f32_kernel(const __grid_constant__ Sp
             if (v) atomicAdd(job.counters + i, v);
         }
     }
+}
+
+template <int DMAX, bool PROD, bool RSMEM, int MAXT>
+__global__ void __launch_bounds__(MAXT) sp_f32_kernel(const __grid_constant__ SpTables tb, const __grid_constant__ SpJob job) {
+    extern __shared__ float sm_f[];
+    const long long lo = job.ncw * blockIdx.x / gridDim.x, hi = job.ncw * (blockIdx.x + 1) / gridDim.x;
+    sp_decode_range<DMAX, PROD, RSMEM>(tb, job, lo, hi, sm_f,
+                                       RSMEM ? nullptr : job.r_scratch + (long long)blockIdx.x * tb.E * blockDim.x);
 }
 
 }  // namespace ldpc

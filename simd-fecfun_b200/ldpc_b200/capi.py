@@ -285,9 +285,10 @@ class Context:
 
 
 class Batch:
-    """Several codes decoded by one persistent launch (ldpc_batch_*, int8
-    offset min-sum).  ``cfgs`` holds one dict of Context keyword arguments
-    (max_iter, max_row_metric, beta) per code."""
+    """Several codes decoded by one persistent launch (ldpc_batch_*).
+    ``cfgs`` holds one dict of Context keyword arguments (variant, max_iter,
+    max_row_metric, beta) per code; every code of a batch uses the same
+    variant (int8 offset min-sum, or one of the float decoders)."""
 
     def __init__(self, codes: Sequence["Code"], cfgs: Sequence[dict], device: int = 0):
         if len(codes) != len(cfgs):
@@ -296,8 +297,8 @@ class Batch:
         arr = (_vp * len(codes))(*[c.h for c in codes])
         cf = (Cfg * len(codes))()
         for i, k in enumerate(cfgs):
-            cf[i] = Cfg(LDPC_INT8_OMS, k.get("max_iter", 10), k.get("max_row_metric", 31.0), k.get("beta", 1.0),
-                        k.get("llr_scale", 2.0), k.get("max_abs_llr", 24.0))
+            cf[i] = Cfg(k.get("variant", LDPC_INT8_OMS), k.get("max_iter", 10), k.get("max_row_metric", 31.0),
+                        k.get("beta", 1.0), k.get("llr_scale", 2.0), k.get("max_abs_llr", 24.0))
         h = _vp()
         check(lib.ldpc_batch_create(arr, cf, len(codes), device, C.byref(h)))
         self.h = h

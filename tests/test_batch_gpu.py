@@ -161,3 +161,56 @@ def test_empty_and_invalid_jobs(capi):
         batch.plan([dict(code=1, llr=llr, n=4)])
     with pytest.raises(capi.LdpcError):
         capi.Batch([h], [dict(beta=200.0)])
+
+
+def _float_llr(oracle, code, n, snr, seed):
+    rng = np.random.default_rng(seed)
+    info = rng.integers(0, 2, (n, (code.mcol - code.mrow) * code.z), dtype=np.uint8)
+    cw = oracle.encode(code, info)
+    noise = rng.standard_normal(cw.shape, dtype=np.float32)
+    lf, _, _ = oracle.llr_array(code, cw, noise, snr, 1.0, 1e9)
+    return lf
+
+
+@pytest.mark.parametrize("mode", [1, 0])
+def test_float_batch_mixed_lifting_sizes(capi, oracle, mode):
+    """802.16e 1/2 at Z = 24, 52, 76, 96 in one float launch (sum-product or
+    offset min-sum), plus 802.11ad 1/2; each codeword bit-exact with the
+    oracle on its own code; then replayed from a CUDA graph."""
+    import torch
+    from ldpc_b200 import codes
+    variant = capi.LDPC_F32_SP if mode == 1 else capi.LDPC_F32_OMS
+    mrm, beta = (6e-8, 0.0) if mode == 1 else (31.0, 0.5)
+    objs = [codes.make_code("16e 1/2", z_over=z) for z in (24, 52, 76, 96)] + [codes.make_code("11ad 1/2")]
+    counts = [300, 170, 90, 257, 333]
+    handles = [capi.Code.from_tables(c) for c in objs]
+    batch = capi.Batch(handles, [dict(variant=variant, max_iter=10, max_row_metric=mrm, beta=beta)] * len(objs))
+    specs, data = [], []
+    for i, (c, h, n) in enumerate(zip(objs, handles, counts)):
+        llr = _float_llr(oracle, c, n, 1.25 if i < 4 else -0.5, 10 + i)
+        b = dict(llr=torch.from_numpy(llr).cuda(), post=torch.empty((n, c.n), dtype=torch.float32, device="cuda"),
+                 iters=torch.empty(n, dtype=torch.uint8, device="cuda"))
+        specs.append(dict(code=i, n=n, **b))
+        data.append(llr)
+    plan = batch.plan(specs)
+    for launch in (plan.launch, plan.graph_launch, plan.graph_launch):
+        for sp in specs:
+            sp["post"].zero_()
+            sp["iters"].fill_(255)
+        torch.cuda.synchronize()
+        launch(torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        for c, sp, llr in zip(objs, specs, data):
+            post_o, it_o = oracle.decode_f32(c, llr, mode, 10, mrm, beta)
+            assert np.array_equal(sp["iters"].cpu().numpy(), it_o.astype(np.uint8))
+            assert np.array_equal(sp["post"].cpu().numpy().view(np.uint32), post_o.view(np.uint32))
+
+
+def test_batch_variants_must_agree(capi):
+    from ldpc_b200 import codes
+    h = capi.Code.from_tables(codes.make_code("11ad 1/2"))
+    with pytest.raises(capi.LdpcError):
+        capi.Batch([h, h], [dict(), dict(variant=capi.LDPC_F32_SP, max_row_metric=6e-8, beta=0.0)])
+    fb = capi.Batch([h], [dict(variant=capi.LDPC_F32_OMS)])
+    with pytest.raises(capi.LdpcError):
+        fb.set_offsets(0, np.ones(8, np.float32))
