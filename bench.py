@@ -236,7 +236,8 @@ def run_workload(args):
     elif args.workload == "sp-sweep":
         out = workloads.sp_sweep(cw_per_z=args.sp_cw, steps=args.steps, warmup=args.warmup)
     else:
-        out = workloads.learned_run(train_steps=max(args.steps, 2), batch=args.learned_batch)
+        out = workloads.learned_run(train_steps=max(args.steps, 2), batch=args.learned_batch,
+                                    weights=args.learned_weights)
     out["clocks"] = _clock_summary(clk)
     print(json.dumps(out), flush=True)
     return 0
@@ -261,6 +262,7 @@ def main():
     ap.add_argument("--llr-budget-gb", type=float, default=40.0, help="nr-mix: LLR bytes the codeword counts are scaled to")
     ap.add_argument("--no-autotune", action="store_true", help="nr-mix: default launch shape")
     ap.add_argument("--learned-batch", type=int, default=65536)
+    ap.add_argument("--learned-weights", default="uniform", choices=["uniform", "early"])
     ap.add_argument("--sp-cw", type=int, default=1 << 20, help="sp-sweep: codewords per Z")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -230,7 +230,11 @@ def hetero_mix(steps: int = 3, warmup: int = 1, total: int = 10_000_000, seed: i
     }
 
 
-def learned_run(train_steps: int = 30, batch: int = 65536, eval_n: int = 200_000, seed: int = 3) -> Dict:
+def learned_run(train_steps: int = 30, batch: int = 65536, eval_n: int = 200_000, seed: int = 3,
+                weights: str = "uniform") -> Dict:
+    """``weights``: "uniform" (every iteration's BCE counts once) or "early"
+    (iteration it weighted 1/(it+1), rewarding codewords that are right
+    sooner)."""
     code = codes.make_code("16e 1/2", z_over=96)
     h = capi.Code.from_tables(code)
     ctx = capi.Context(h, variant=capi.LDPC_F32_OMS, max_iter=10, max_row_metric=31.0, beta=0.5, llr_scale=1.0,
@@ -240,8 +244,9 @@ def learned_run(train_steps: int = 30, batch: int = 65536, eval_n: int = 200_000
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
+    lw = [1.0 / (i + 1) for i in range(10)] if weights == "early" else None
     beta, hist = learned.train(ctx, code, iters=10, batch=batch, steps=train_steps, ebn0=(1.0, 2.5), lr=0.01,
-                               init=0.5, seed=seed)
+                               init=0.5, seed=seed, loss_w=lw)
     e1.record()
     torch.cuda.synchronize()
     train_ms = e0.elapsed_time(e1)
@@ -260,7 +265,8 @@ def learned_run(train_steps: int = 30, batch: int = 65536, eval_n: int = 200_000
     fb_ms = sorted(a.elapsed_time(c) for a, c in ev)[2]
     plain = torch.full_like(beta, 0.5)
     evals = []
-    for eb in (0.0, 1.0, 1.5, 2.0):
+    # Eb/N0 points; 3.01 dB is the reference's SNR (Es/N0) of 0 dB at rate 1/2
+    for eb in (0.0, 1.0, 1.5, 2.0, 2.5, 3.01):
         snr = learned.snr_from_ebn0(eb, 0.5)
         cp, bp, ip = learned.evaluate(ctx, code, plain, snr, eval_n)
         cl, bl, il = learned.evaluate(ctx, code, beta, snr, eval_n)
@@ -273,8 +279,8 @@ def learned_run(train_steps: int = 30, batch: int = 65536, eval_n: int = 200_000
         "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: codewords drawn on the device by the library's generator every step",
         "config": {"workload": "802.16e 1/2 Z=96 (N=2304), batches of %d codewords, Eb/N0 uniform in [1.0, 2.5] dB "
-                               "(16 points per batch), 120 offsets from 0.5, Adam lr 0.01, BCE over all iterations"
-                               % batch,
+                               "(16 points per batch), 120 offsets from 0.5, Adam lr 0.01, BCE over all iterations "
+                               "(%s weights)" % (batch, weights),
                    "step": "generation + encoding + forward with checkpoints + adjoint + Adam"},
         "forward_adjoint_ms": fb_ms,
         "forward_adjoint_cw_s": batch / (fb_ms * 1e-3),
