@@ -357,11 +357,18 @@ def main():
     peak = capi.probe_int32_peak(local)
     bytes_per_cw = N + 4 * HW + 1
     traffic = None
+    pipe = None
     prof = os.path.join(ROOT, "profiles", "decode_11ad_traffic.json")
     if os.path.exists(prof):
         with open(prof) as f:
             p = json.load(f)
         traffic = p["dram_bytes_per_codeword"] * total
+        if "alu_pipe_pct" in p:
+            # what the hardware executes, beside the 2.5-op-per-edge definition of "achieved"
+            pipe = {"alu_pipe_active": p["alu_pipe_pct"] / 100, "issue_active": p["issue_active_pct"] / 100,
+                    "thread_instructions_per_edge_per_codeword": p["warp_instructions"] * 32.0
+                    / (p["codeword_iterations"] * p["edges_per_codeword"]),
+                    "source": "ncu --set full of this kernel (profiles/oms_f16_11ad_small_ncu.md)"}
     roofline = {
         "bound": "alu", "achieved": ops_per_launch / avg_launch_s / 1e12, "peak": peak / 1e12, "unit": "Tops/s (int32)",
         "frac": ops_per_launch / avg_launch_s / peak, "traffic": traffic,
@@ -370,6 +377,8 @@ def main():
                           "edge-iteration, 4 lanes per 32-bit op)",
         "hbm": {"achieved_gbs": bytes_per_cw * total / avg_launch_s / 1e9, "bytes_per_codeword": bytes_per_cw},
     }
+    if pipe:
+        roofline["pipe"] = pipe
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             hbm_peak = json.load(f)["hbm_gbs"]
