@@ -104,6 +104,15 @@ void ldpc_code_destroy(ldpc_code *code);
 int ldpc_ctx_create(const ldpc_code *code, const ldpc_cfg *cfg, int device, ldpc_ctx **out);
 void ldpc_ctx_destroy(ldpc_ctx *ctx);
 
+/* int8 contexts: one offset per layer (beta_per_layer[mrow], truncated to
+ * int8 like cfg.beta) in place of cfg.beta on every layer, e.g. learned
+ * offsets quantised to the int8 LLR scale.  NULL restores cfg.beta.  The
+ * reference applies one offset to all layers (decode_functions.cpp:59-62).
+ * Decoding then runs on the run-time-table kernel.  The call waits for the
+ * device to be idle, so it is not for use between asynchronous launches in
+ * flight. */
+int ldpc_ctx_set_layer_offsets(ldpc_ctx *ctx, const float *beta_per_layer);
+
 /* ---- decoding ------------------------------------------------------------- */
 
 /* Decode n codewords of int8 LLRs (variant LDPC_INT8_OMS).  Replaces

@@ -326,6 +326,29 @@ int ldpc_ctx_create(const ldpc_code* code, const ldpc_cfg* cfg, int device, ldpc
     return LDPC_OK;
 }
 
+int ldpc_ctx_set_layer_offsets(ldpc_ctx* x, const float* beta) {
+    if (!x) return fail(LDPC_ERR_INVALID_ARG, "ctx is NULL");
+    if (x->cfg.variant != LDPC_INT8_OMS) return fail(LDPC_ERR_UNSUPPORTED, "per-layer offsets are for int8 contexts");
+    std::vector<int> table;
+    if (beta) {
+        for (int l = 0; l < x->code.mrow; ++l) {
+            if (!(beta[l] >= 0.0f && beta[l] < 128.0f))
+                return fail(LDPC_ERR_UNSUPPORTED, "offset %g of layer %d outside [0, 128)", beta[l], l);
+            table.push_back((int)(int8_t)beta[l]);   // truncated like cfg.beta (decode_functions.cpp:60)
+        }
+    }
+    CUDA_TRY(cudaSetDevice(x->device));
+    CUDA_TRY(cudaDeviceSynchronize());   // no launch of this context may still use the old descriptor
+    cudaFree(x->d_rt_code);
+    cudaFree(x->d_rt_scratch);
+    x->d_rt_code = nullptr;
+    x->d_rt_scratch = nullptr;
+    x->oms_rt = false;
+    x->inst = nullptr;
+    x->layer_beta8 = table;
+    return ldpc::setup_oms(x);
+}
+
 void ldpc_ctx_destroy(ldpc_ctx* x) {
     if (!x) return;
     cudaSetDevice(x->device);

@@ -96,9 +96,12 @@ int setup_oms_rt(ldpc_ctx* x) {
     if (smem > (size_t)kRtMaxSmem)
         return fail(LDPC_ERR_UNSUPPORTED, "int8 decoder: N=%d needs %zu B of shared memory", n, smem);
     RtCode host;
-    int rc = make_rt_code(c, (int)x->cfg.max_iter, x->maxv2, nullptr, (int)(int8_t)x->cfg.beta, G, &host);
+    const int* table = x->layer_beta8.empty() ? nullptr : x->layer_beta8.data();
+    int rc = make_rt_code(c, (int)x->cfg.max_iter, x->maxv2, table, (int)(int8_t)x->cfg.beta, G, &host);
     if (rc) return rc;
-    rt_fn k = rt_kernel_for(dmax, x->beta0, rsmem);
+    bool quirk = x->layer_beta8.empty() && x->beta0;
+    for (int v : x->layer_beta8) quirk |= v == 0;
+    rt_fn k = rt_kernel_for(dmax, quirk, rsmem);
     CUDA_TRY(allow_dynamic_smem((const void*)k, kRtMaxSmem));
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k, threads, smem));

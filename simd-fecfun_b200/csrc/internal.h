@@ -95,6 +95,7 @@ struct ldpc_ctx {
     int oms_threads = 0, oms_smem = 0, oms_ctas = 0;
     uint32_t beta2 = 0, maxv2 = 0;
     bool beta0 = false;
+    std::vector<int> layer_beta8;               // per-layer int8 offsets (ldpc_ctx_set_layer_offsets), empty = cfg.beta
     int oms_synd_loop = 0;                      // syndrome as a table loop (tuning: LDPC_OMS_SYND_LOOP)
     // int8 offset min-sum over run-time tables (shapes without a compiled kernel)
     bool oms_rt = false;

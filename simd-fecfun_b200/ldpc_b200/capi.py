@@ -74,6 +74,7 @@ _PROTOS = {
     "ldpc_code_destroy": (None, [_vp]),
     "ldpc_ctx_create": (C.c_int, [_vp, C.POINTER(Cfg), C.c_int, C.POINTER(_vp)]),
     "ldpc_ctx_destroy": (None, [_vp]),
+    "ldpc_ctx_set_layer_offsets": (C.c_int, [_vp, _vp]),
     "ldpc_decode_int8": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _vp]),
     "ldpc_decode_f32": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _vp]),
     "ldpc_decode_int16": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _vp]),
@@ -213,6 +214,14 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def set_layer_offsets(self, beta_per_layer=None):
+        """int8 contexts: one offset per layer (None restores cfg.beta)."""
+        if beta_per_layer is None:
+            check(lib.ldpc_ctx_set_layer_offsets(self.h, None))
+            return
+        b = np.ascontiguousarray(beta_per_layer, dtype=np.float32)
+        check(lib.ldpc_ctx_set_layer_offsets(self.h, b.ctypes.data))
 
     # ---- device-pointer API (torch tensors) ----
     def decode_int8(self, llr, n, post=None, hard=None, iters=None, stream=0):

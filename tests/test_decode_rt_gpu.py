@@ -188,3 +188,24 @@ def test_nr_generate_and_simulate(capi):
     assert not bits[:, fs:fe + 1].any()
     st = ctx.simulate(seed=3, cw_offset=0, snr_db=[-3.0], n_per_snr=2000)[0]
     assert st["codewords"] == 2000 and st["cw_errors"] == 0 and st["iterations"] >= 2000
+
+
+@pytest.mark.parametrize("name,snr", [("11ad 1/2", -0.5), ("5GNR_n1000_k500", -1.0)])
+def test_context_layer_offsets(capi, oracle, name, snr):
+    """ldpc_ctx_set_layer_offsets: one int8 offset per layer (0 included),
+    then back to cfg.beta (for 11ad, back onto the compiled kernel)."""
+    from ldpc_b200 import codes
+    code = codes.code_by_name(name)
+    llr, _, _ = make_llr_int8(code, 400, snr, seed=31, oracle=oracle)
+    ctx = capi.Context(capi.Code.from_tables(code), max_iter=12, beta=1.0)
+    b = np.arange(code.mrow, dtype=np.float32) % 4 + np.float32(0.5)      # truncated to 0..3
+    ctx.set_layer_offsets(b)
+    post, hard, iters, tot = ctx.decode_host(llr)
+    post_o, it_o = oracle.decode_int8(code, llr, 12, 31.0, beta_layers=b.astype(np.int8))
+    assert np.array_equal(post, post_o) and np.array_equal(iters, it_o.astype(np.uint8))
+    ctx.set_layer_offsets(None)
+    post, hard, iters, tot = ctx.decode_host(llr)
+    post_o, it_o = oracle.decode_int8(code, llr, 12, 31.0, 1.0)
+    assert np.array_equal(post, post_o) and np.array_equal(iters, it_o.astype(np.uint8))
+    with pytest.raises(capi.LdpcError):
+        ctx.set_layer_offsets(np.full(code.mrow, 300.0, np.float32))
