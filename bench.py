@@ -218,6 +218,80 @@ def run_reference(args):
     return 0
 
 
+def ref_variant_rate(build, mrm, beta, scale, max_abs, threads, per, snrs, max_iter=10):
+    """One reference build (oracle/_ref/libref_<build>.so) on host threads:
+    inputs through the reference's own pipeline (normdist2,
+    gen_rand_databits, LDPCencode, gen_metrics) with the SNR points assigned
+    to threads in rotation, untimed; then LDPCdecode_set on every thread at
+    once, timed.  Returns (codewords/s, average iterations) or None when the
+    build is absent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import refbind as rb
+    from ldpc_b200 import codes
+    if not rb.ref_available(build):
+        return None
+    lib = rb.RefLib(build)
+    code = codes.make_code(CODE, elem_size=abs(lib.elem_bw))
+    ctxs = []
+    for k in range(threads):
+        with _quiet_stdout():
+            c = rb.RefCtx(lib, code, per)
+        seeds = (np.arange(64, dtype=np.uint64) + np.uint64(2000 + k)) * np.uint64(0x9E3779B97F4A7C15) | np.uint64(1)
+        rb.ref_init_randstate(lib, seeds)
+        wgn = rb.ref_normdist2(lib, c.wgn_count())
+        c.gen_rand_databits()
+        c.encode()
+        c.gen_metrics(snrs[k % len(snrs)], wgn, scale, max_abs)
+        ctxs.append(c)
+    t0 = [0.0] * threads
+    t1 = [0.0] * threads
+    its = [0] * threads
+
+    def work(k):
+        t0[k] = time.perf_counter()
+        its[k] = ctxs[k].decode_set(max_iter, mrm, beta)
+        t1[k] = time.perf_counter()
+
+    th = [threading.Thread(target=work, args=(k,)) for k in range(threads)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    return threads * per / (max(t1) - min(t0)), sum(its) / (threads * per)
+
+
+def run_variants(args, clk):
+    """--workload variants: every decoder variant on the headline 802.11ad
+    simulation point, GPU device time beside the reference build of the same
+    variant on this box's host cores."""
+    from ldpc_b200 import workloads
+    rows = workloads.variants(n_per_snr=args.variant_n)
+    threads = os.cpu_count() or 1
+    for r, run in zip(rows, workloads.VARIANT_RUNS):
+        _, _, build, mrm, beta, scale, max_abs = run
+        # a bounded CPU sample: fewer codewords for the slower element types
+        per = max(64, int(args.variant_ref_sample * {"c": 1.0, "s": 0.5, "w": 0.25, "f": 0.25, "d": 0.1}[build.split("_")[0][-1]]))
+        rr = ref_variant_rate(build, mrm, beta, scale, max_abs, threads, per, SNRS)
+        if rr is not None:
+            r["cpu_reference"] = {"value": rr[0], "unit": "codewords/s", "cores": threads, "kind": "reference",
+                                  "avg_iter": rr[1], "sample": "%d codewords x %d threads" % (per, threads)}
+            r["speedup_vs_cpu_reference"] = r["value"] / rr[0]
+    dsp = rows[-1]
+    return {
+        "metric": "codewords/s decoded, 802.11ad rate-1/2, each decoder variant, 10 max iterations",
+        "value": dsp["value"], "value_is": "double sum-product (the slowest variant); every variant under 'variants'",
+        "unit": "codewords/s", "n_gpus": 1, "steps": 1, "warmup": 1, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "per variant",
+        "data": "synthetic: Philox data bits + AWGN from the fused generator, LLRs of each variant's element type",
+        "config": {"workload": "802.11ad rate 1/2, SNR -1.00..0.00 dB step 0.25, %d codewords per SNR per variant; "
+                               "the Perl driver's parameters per variant" % args.variant_n,
+                   "timing": "decoder device time only (CUDA events around each launch in ldpc_simulate)"},
+        "gpu_launches": 2 * len(rows) * len(SNRS),
+        "variants": rows,
+    }
+
+
 def run_workload(args):
     """The other measured workloads (ldpc_b200.workloads), on one GPU; under
     torchrun only rank 0 runs."""
@@ -235,6 +309,8 @@ def run_workload(args):
         out = workloads.hetero_mix(steps=args.steps, warmup=args.warmup)
     elif args.workload == "sp-sweep":
         out = workloads.sp_sweep(cw_per_z=args.sp_cw, steps=args.steps, warmup=args.warmup)
+    elif args.workload == "variants":
+        out = run_variants(args, clk)
     else:
         out = workloads.learned_run(train_steps=max(args.steps, 2), batch=args.learned_batch,
                                     weights=args.learned_weights)
@@ -255,10 +331,14 @@ def main():
     ap.add_argument("--cpu-reps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="11ad", choices=["11ad", "nr-mix", "hetero-mix", "learned", "sp-sweep"],
+    ap.add_argument("--variant-n", type=int, default=200_000, help="codewords per SNR per variant (--workload variants)")
+    ap.add_argument("--variant-ref-sample", type=int, default=4000,
+                    help="int8 codewords per host thread for the reference builds (--workload variants)")
+    ap.add_argument("--workload", default="11ad",
+                    choices=["11ad", "nr-mix", "hetero-mix", "learned", "sp-sweep", "variants"],
                     help="11ad: the headline run; others: the batched 5G NR mix, the 18-code 802.11 mix "
-                         "(plain vs learned offsets), learned-offset training, the float sum-product Z sweep "
-                         "(one GPU)")
+                         "(plain vs learned offsets), learned-offset training, the float sum-product Z sweep, "
+                         "every decoder variant on the headline point (one GPU)")
     ap.add_argument("--llr-budget-gb", type=float, default=40.0, help="nr-mix: LLR bytes the codeword counts are scaled to")
     ap.add_argument("--no-autotune", action="store_true", help="nr-mix: default launch shape")
     ap.add_argument("--learned-batch", type=int, default=65536)

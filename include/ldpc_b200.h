@@ -45,7 +45,9 @@ enum {
     LDPC_F32_SP = 1,            /* float sum-product     (LDPCtop_Vec16f_prod) */
     LDPC_F32_OMS = 2,           /* float offset min-sum  (LDPCtop_Vec16f_min)  */
     LDPC_INT16_OMS = 3,         /* int16 offset min-sum  (LDPCtop_Vec32s_min)  */
-    LDPC_INT32_OMS = 4          /* int32 offset min-sum  (LDPCtop_Vec16w_min)  */
+    LDPC_INT32_OMS = 4,         /* int32 offset min-sum  (LDPCtop_Vec16w_min)  */
+    LDPC_F64_SP = 5,            /* double sum-product    (LDPCtop_Vec8d_prod)  */
+    LDPC_F64_OMS = 6            /* double offset min-sum (LDPCtop_Vec8d_min)   */
 };
 
 typedef struct ldpc_code ldpc_code;
@@ -67,7 +69,7 @@ typedef struct {
  * (sim_struct_LDPC.h:3-20) plus the variant, which the reference selects at
  * compile time (build/Makefile:9-14). */
 typedef struct {
-    int variant;                /* LDPC_INT8_OMS / LDPC_F32_SP / LDPC_F32_OMS / LDPC_INT16_OMS / LDPC_INT32_OMS */
+    int variant;                /* one of the LDPC_* variants above */
     unsigned max_iter;          /* maximum decoder iterations (1..255) */
     float max_row_metric;       /* min-sum clamp, or 1-clamp for sum-product */
     float beta;                 /* offset (truncated to the element type for the integer variants) */
@@ -131,6 +133,14 @@ int ldpc_decode_int8(ldpc_ctx *ctx, const int8_t *llr, size_t n, int8_t *post_ou
 int ldpc_decode_f32(ldpc_ctx *ctx, const float *llr, size_t n, float *post_out, uint32_t *hard_out,
                     uint8_t *iters_out, void *stream);
 
+/* Double decoders (LDPC_F64_SP, LDPC_F64_OMS): same contract, double LLRs
+ * and posteriors.  The reference's double builds take the float LLRs of
+ * gen_metrics widened to double (gen_metrics.cpp:91-93); beta and
+ * max_row_metric convert to double as decode_row does (decode_functions.cpp:27-32,
+ * 59-60). */
+int ldpc_decode_f64(ldpc_ctx *ctx, const double *llr, size_t n, double *post_out, uint32_t *hard_out,
+                    uint8_t *iters_out, void *stream);
+
 /* int16 / int32 decoders (LDPC_INT16_OMS / LDPC_INT32_OMS): same contract,
  * LLRs and posteriors of the element type.  The reference's element
  * semantics hold: saturating add/sub, abs of the most negative value is
@@ -157,6 +167,8 @@ int ldpc_decode_count(ldpc_ctx *ctx, const void *llr, size_t n, uint32_t *hard_o
 int ldpc_decode_int8_host(ldpc_ctx *ctx, const int8_t *llr, size_t n, int8_t *post_out, uint32_t *hard_out,
                           uint8_t *iters_out, uint64_t *tot_iter);
 int ldpc_decode_f32_host(ldpc_ctx *ctx, const float *llr, size_t n, float *post_out, uint32_t *hard_out,
+                         uint8_t *iters_out, uint64_t *tot_iter);
+int ldpc_decode_f64_host(ldpc_ctx *ctx, const double *llr, size_t n, double *post_out, uint32_t *hard_out,
                          uint8_t *iters_out, uint64_t *tot_iter);
 int ldpc_decode_int16_host(ldpc_ctx *ctx, const int16_t *llr, size_t n, int16_t *post_out, uint32_t *hard_out,
                            uint8_t *iters_out, uint64_t *tot_iter);
@@ -272,8 +284,10 @@ int ldpc_learned_decode(ldpc_ctx *ctx, const float *llr, size_t n, int iters, co
  * so every SNR point sees the same data and the same noise, scaled by its
  * sigma, as the reference's inner loop does (LDPCtop.cpp:89-97).
  * Outputs (dev):
- *   llr_int or llr_f32 [n_snr][n_per_snr][N]   (one of them, by variant: llr_int
- *                      holds int8, int16 or int32 elements, the context's type)
+ *   llr_int or llr_f32 [n_snr][n_per_snr][N]   (either or both: llr_int holds
+ *                      elements of the context's type -- int8, int16, int32,
+ *                      or double for the LDPC_F64_* variants, the float LLRs
+ *                      widened; llr_f32 the float LLRs)
  *   data_bits          [n_per_snr][hard_words] sent data bits (optional)
  *   uncoded_err        [n_snr] sign errors before decoding (optional,
  *                      accumulated: caller zeroes)                         */
@@ -282,7 +296,8 @@ int ldpc_generate(ldpc_ctx *ctx, uint64_t seed, uint64_t cw_offset, const float 
                   unsigned long long *uncoded_err, void *stream);
 
 /* LLR quantisation of given noise (dev): cw_bits [n][N] 0/1 bytes,
- * noise [n][N] float -> llr [n][N] (int8 or float by variant) at one SNR.
+ * noise [n][N] float -> llr [n][N] (llr_int in the context's element type,
+ * llr_f32 float; float contexts fill llr_f32 only) at one SNR.
  * Bit-exact restatement of gen_metrics(); used for parity checks. */
 int ldpc_llr_from_noise(ldpc_ctx *ctx, const uint8_t *cw_bits, const float *noise, size_t n, float snr_db,
                         void *llr_int, float *llr_f32, unsigned long long *uncoded_err, void *stream);

@@ -215,6 +215,98 @@ int orc_decode_f32(const orc_code *c, const orc_trees *tr, int mode, const float
     return 0;
 }
 
+/* The float decoder in double precision: the reference's SIMD_ELEM_BW=-64
+ * builds (LDPCtop_Vec8d_prod / Vec8d_min).  decode_row's operations are
+ * unchanged, on double lanes: Q = P - R, a = max(|Q| - (double)beta, 0)
+ * (decode_functions.cpp:53-62), tanh(a * 0.5) (min_find.pl:38), the product
+ * or min tree with the clamp min(Max_val, .) at Max_val = 1.0 -
+ * (double)max_row_metric below 1e-6 else (double)max_row_metric
+ * (decode_functions.cpp:27-32, min_find.pl:99-107), 2.0 * atanh(.)
+ * (min_find.pl:44), sign_combine and P = Q + R' (:85-91).  tanh/atanh are the
+ * shared lmd_tanh / lmd_atanh. */
+static uint64_t dbits(double x) { uint64_t u; memcpy(&u, &x, 8); return u; }
+static double bitsd(uint64_t u) { double x; memcpy(&x, &u, 8); return x; }
+
+static void run_tree_f64(const int32_t *prog, int len, int d, int prod, const double *in, double maxv, double *node,
+                         double *out) {
+    for (int j = 0; j < d; ++j) node[j] = in[j];
+    for (int k = 0; k < len; ++k) {
+        const int32_t *q = prog + 4 * k;
+        if (q[0] == 0) {
+            double a = node[q[2]], b = node[q[3]];
+            node[q[1]] = prod ? a * b : (a < b ? a : b);
+        } else if (q[0] == 1) {
+            node[q[1]] = maxv < node[q[1]] ? maxv : node[q[1]];
+        } else {
+            out[q[1]] = node[q[2]];
+        }
+    }
+}
+
+int orc_decode_f64(const orc_code *c, const orc_trees *tr, int mode, const double *llr, size_t n_cw,
+                   unsigned max_iter, float max_row_metric, float beta, double *post_out, uint32_t *iters_out) {
+    const int z = c->z, n = z * c->mcol, E = total_edges(c), dmax = max_weight(c);
+    const double maxv = max_row_metric < 1e-6 ? 1.0 - (double)max_row_metric : (double)max_row_metric;
+    const double b = (double)beta;
+    if (dmax > tr->max_d) return -1;
+    double *P = (double *)malloc(sizeof(double) * (size_t)n);
+    double *R = (double *)malloc(sizeof(double) * (size_t)E * z);
+    double *Q = (double *)malloc(sizeof(double) * (size_t)dmax), *x = (double *)malloc(sizeof(double) * (size_t)dmax);
+    double *f = (double *)malloc(sizeof(double) * (size_t)dmax);
+    double *node = (double *)malloc(sizeof(double) * ((size_t)dmax * 8 + 64));
+    int *v = (int *)malloc(sizeof(int) * (size_t)dmax);
+    for (size_t cw = 0; cw < n_cw; ++cw) {
+        memcpy(P, llr + cw * (size_t)n, sizeof(double) * (size_t)n);
+        memset(R, 0, sizeof(double) * (size_t)E * z);
+        unsigned iter = 0;
+        int done = 0;
+        while (!done) {
+            int e0 = 0;
+            for (int r = 0; r < c->mrow; ++r) {
+                const int d = c->row_weights[r];
+                for (int t = 0; t < z; ++t) {
+                    uint64_t rx = 0;
+                    for (int j = 0; j < d; ++j) {
+                        const int col = c->row_cols[e0 + j], s = c->row_shifts[e0 + j];
+                        v[j] = col * z + (s + t) % z;
+                        Q[j] = P[v[j]] - R[(size_t)(e0 + j) * z + t];
+                        double a = fabs(Q[j]) - b;
+                        a = a > 0.0 ? a : 0.0;
+                        x[j] = mode ? lmd_tanh(a * 0.5) : a;
+                        rx ^= dbits(Q[j]);
+                    }
+                    run_tree_f64(tr->prog + 4 * tr->off[d], tr->len[d], d, mode, x, maxv, node, f);
+                    for (int j = 0; j < d; ++j) {
+                        double fj = mode ? 2.0 * lmd_atanh(f[j]) : f[j];
+                        uint64_t s = (rx ^ dbits(Q[j])) & 0x8000000000000000ULL;
+                        double rn = bitsd(dbits(fj) ^ s);
+                        P[v[j]] = Q[j] + rn;
+                        R[(size_t)(e0 + j) * z + t] = rn;
+                    }
+                }
+                e0 += d;
+            }
+            int bad = 0;
+            e0 = 0;
+            for (int r = 0; r < c->mrow && !bad; ++r) {
+                const int d = c->row_weights[r];
+                for (int t = 0; t < z; ++t) {
+                    uint64_t xx = 0;
+                    for (int j = 0; j < d; ++j) xx ^= dbits(P[c->row_cols[e0 + j] * z + (c->row_shifts[e0 + j] + t) % z]);
+                    if (xx & 0x8000000000000000ULL) { bad = 1; break; }
+                }
+                e0 += d;
+            }
+            ++iter;
+            done = !bad || iter == max_iter;
+        }
+        if (post_out) memcpy(post_out + cw * (size_t)n, P, sizeof(double) * (size_t)n);
+        if (iters_out) iters_out[cw] = iter;
+    }
+    free(P); free(R); free(Q); free(x); free(f); free(node); free(v);
+    return 0;
+}
+
 /* int8 decoding through the generated min tree instead of the direct
  * exclusive minimum (identical by exactness of integer min; kept to check it) */
 int orc_decode_int8_tree(const orc_code *c, const orc_trees *tr, const int8_t *llr, size_t n_cw,

@@ -52,6 +52,11 @@ int orc_decode_f32(const orc_code *c, const orc_trees *t, int mode, const float 
                    unsigned max_iter, float max_row_metric, float beta, float *post_out,
                    uint32_t *iters_out);
 
+/* the same decoder in double precision (the reference's Vec8d builds) */
+int orc_decode_f64(const orc_code *c, const orc_trees *t, int mode, const double *llr, size_t n_cw,
+                   unsigned max_iter, float max_row_metric, float beta, double *post_out,
+                   uint32_t *iters_out);
+
 /* sigma and LLR factor exactly as gen_metrics.cpp:26-30 computes them */
 void orc_sigma(float snr, float llr_scale, float *sigma, float *sigma_factor);
 

@@ -236,6 +236,20 @@ class Oracle:
             raise RuntimeError("orc_decode_f32 failed (row weight above the tree table)")
         return post, it
 
+    def decode_f64(self, code, llr, mode=1, max_iter=10, max_row_metric=6e-8, beta=0.0):
+        llr = np.ascontiguousarray(llr, dtype=np.float64).reshape(-1, code.n)
+        n = llr.shape[0]
+        post = np.zeros_like(llr)
+        it = np.zeros(n, np.uint32)
+        cs, keep = self._code(code)
+        rc = self.lib.orc_decode_f64(C.byref(cs), C.byref(self._tree_struct()), C.c_int(mode),
+                                     llr.ctypes.data_as(C.c_void_p), C.c_size_t(n), C.c_uint(max_iter),
+                                     C.c_float(max_row_metric), C.c_float(beta), post.ctypes.data_as(C.c_void_p),
+                                     it.ctypes.data_as(C.c_void_p))
+        if rc != 0:
+            raise RuntimeError("orc_decode_f64 failed (row weight above the tree table)")
+        return post, it
+
     def sigma(self, snr, llr_scale):
         s, f = C.c_float(), C.c_float()
         self.lib.orc_sigma(C.c_float(snr), C.c_float(llr_scale), C.byref(s), C.byref(f))
@@ -299,6 +313,8 @@ class Oracle:
 
     def count_errors(self, code, post, cw_bits):
         post = np.ascontiguousarray(post)
+        if post.dtype in (np.float64, np.int16, np.int32):
+            post = np.where(post < 0, -1, 1).astype(np.int8)     # only the signs are counted
         cw_bits = np.ascontiguousarray(cw_bits, dtype=np.uint8)
         n = post.shape[0]
         a, b = C.c_uint64(), C.c_uint64()

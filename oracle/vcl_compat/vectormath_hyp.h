@@ -1,9 +1,9 @@
 /* vectormath_hyp.h -- compatibility header (oracle / CPU-baseline only).
  *
  * The reference's sum-product tree (src/LDPCDec/min_find.pl:37-48,98-106)
- * calls tanh() and atanh() on float vectors from vectorclass's
+ * calls tanh() and atanh() on float (and double) vectors from vectorclass's
  * vectormath_hyp.h, which is absent here.  Both are mapped lane by lane onto
- * the project's shared float functions (simd-fecfun_b200/csrc/ldpc_math.h),
+ * the project's shared functions (simd-fecfun_b200/csrc/ldpc_math.h),
  * the same code the GPU decoder runs, so the CPU oracle and the GPU agree
  * bit for bit.  This pins parity to that function, not to vectorclass's.
  */
@@ -21,4 +21,14 @@ static inline Vec8f tanh(const Vec8f a) { return vclc_lanewise(a, lm_tanh); }
 static inline Vec16f tanh(const Vec16f a) { return vclc_lanewise(a, lm_tanh); }
 static inline Vec8f atanh(const Vec8f a) { return vclc_lanewise(a, lm_atanh); }
 static inline Vec16f atanh(const Vec16f a) { return vclc_lanewise(a, lm_atanh); }
+/* double lanes (the SIMD_ELEM_BW=-64 builds): the shared double functions */
+template <class V> static inline V vclc_lanewise_d(const V& a, double (*f)(double)) {
+    V r;
+    for (int i = 0; i < V::size(); ++i) r.e[i] = f(a.e[i]);
+    return r;
+}
+static inline Vec4d tanh(const Vec4d a) { return vclc_lanewise_d(a, lmd_tanh); }
+static inline Vec8d tanh(const Vec8d a) { return vclc_lanewise_d(a, lmd_tanh); }
+static inline Vec4d atanh(const Vec4d a) { return vclc_lanewise_d(a, lmd_atanh); }
+static inline Vec8d atanh(const Vec8d a) { return vclc_lanewise_d(a, lmd_atanh); }
 #endif

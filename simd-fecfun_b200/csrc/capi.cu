@@ -269,7 +269,7 @@ int ldpc_ctx_create(const ldpc_code* code, const ldpc_cfg* cfg, int device, ldpc
     *out = nullptr;
     if (cfg->max_iter < 1 || cfg->max_iter > 255)
         return fail(LDPC_ERR_UNSUPPORTED, "max_iter=%u outside 1..255", cfg->max_iter);
-    if (cfg->variant < LDPC_INT8_OMS || cfg->variant > LDPC_INT32_OMS)
+    if (cfg->variant < LDPC_INT8_OMS || cfg->variant > LDPC_F64_OMS)
         return fail(LDPC_ERR_INVALID_ARG, "unknown variant %d", cfg->variant);
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -373,13 +373,20 @@ void ldpc_ctx_destroy(ldpc_ctx* x) {
 
 namespace {
 
-// LLR element kinds of the entry points: 0 int8, 1 float, 2 int16, 3 int32
+// LLR element kinds of the entry points: 0 int8, 1 float, 2 int16, 3 int32, 4 double
 int llr_kind(int variant) {
-    return variant == LDPC_INT8_OMS ? 0 : variant == LDPC_INT16_OMS ? 2 : variant == LDPC_INT32_OMS ? 3 : 1;
+    switch (variant) {
+        case LDPC_INT8_OMS: return 0;
+        case LDPC_INT16_OMS: return 2;
+        case LDPC_INT32_OMS: return 3;
+        case LDPC_F64_SP:
+        case LDPC_F64_OMS: return 4;
+        default: return 1;
+    }
 }
 
 int check_decode_args(ldpc_ctx* x, size_t n, const void* llr, int kind) {
-    static const char* names[] = {"int8", "float", "int16", "int32"};
+    static const char* names[] = {"int8", "float", "int16", "int32", "double"};
     if (!x) return fail(LDPC_ERR_INVALID_ARG, "ctx is NULL");
     if (n && !llr) return fail(LDPC_ERR_INVALID_ARG, "llr is NULL");
     if (llr_kind(x->cfg.variant) != kind)
@@ -498,6 +505,20 @@ int ldpc_decode_f32(ldpc_ctx* x, const float* llr, size_t n, float* post_out, ui
     return ldpc::launch_sp(x, a, (cudaStream_t)stream);
 }
 
+int ldpc_decode_f64(ldpc_ctx* x, const double* llr, size_t n, double* post_out, uint32_t* hard_out, uint8_t* iters_out,
+                    void* stream) {
+    int rc = check_decode_args(x, n, llr, 4);
+    if (rc) return rc;
+    CUDA_TRY(cudaSetDevice(x->device));
+    ldpc::DecodeArgs a;
+    a.llr = llr;
+    a.n = n;
+    a.post = post_out;
+    a.hard = hard_out;
+    a.iters = iters_out;
+    return ldpc::launch_sp(x, a, (cudaStream_t)stream);
+}
+
 int ldpc_decode_count(ldpc_ctx* x, const void* llr, size_t n, uint32_t* hard_out, uint8_t* iters_out,
                       const uint32_t* data_bits, size_t ref_period, size_t bucket_size, unsigned long long* counters,
                       int n_buckets, void* stream) {
@@ -532,6 +553,13 @@ int ldpc_decode_f32_host(ldpc_ctx* x, const float* llr, size_t n, float* post_ou
     int rc = check_decode_args(x, n, llr, 1);
     if (rc) return rc;
     return decode_host<float>(x, llr, n, post_out, hard_out, iters_out, tot_iter);
+}
+
+int ldpc_decode_f64_host(ldpc_ctx* x, const double* llr, size_t n, double* post_out, uint32_t* hard_out,
+                         uint8_t* iters_out, uint64_t* tot_iter) {
+    int rc = check_decode_args(x, n, llr, 4);
+    if (rc) return rc;
+    return decode_host<double>(x, llr, n, post_out, hard_out, iters_out, tot_iter);
 }
 
 int ldpc_decode_int16(ldpc_ctx* x, const int16_t* llr, size_t n, int16_t* post_out, uint32_t* hard_out,
@@ -595,6 +623,7 @@ int ldpc_decode_set_compat(ldpc_ctx* x, void* metrics, unsigned num_cw, unsigned
         case 0: rc = decode_host<int8_t>(x, (const int8_t*)flat.data(), num_cw, (int8_t*)post.data(), nullptr, nullptr, &it); break;
         case 2: rc = decode_host<int16_t>(x, (const int16_t*)flat.data(), num_cw, (int16_t*)post.data(), nullptr, nullptr, &it); break;
         case 3: rc = decode_host<int32_t>(x, (const int32_t*)flat.data(), num_cw, (int32_t*)post.data(), nullptr, nullptr, &it); break;
+        case 4: rc = decode_host<double>(x, (const double*)flat.data(), num_cw, (double*)post.data(), nullptr, nullptr, &it); break;
         default: rc = decode_host<float>(x, (const float*)flat.data(), num_cw, (float*)post.data(), nullptr, nullptr, &it);
     }
     if (rc) return rc;

@@ -1,4 +1,4 @@
-// Host side of the float decoders (sum-product, offset min-sum).
+// Host side of the float and double decoders (sum-product, offset min-sum).
 #include <algorithm>
 #include <cstring>
 
@@ -13,14 +13,17 @@ struct SpVariant {
     int dmax;
     bool prod, rsmem;
     sp_fn k;
+    sp64_fn k64;
 };
-#define SPV(D_, P_, R_) {D_, P_, R_, sp_f32_kernel<D_, P_, R_, SP_MAXT>}
+#define SPV(D_, P_, R_) {D_, P_, R_, sp_f32_kernel<D_, P_, R_, SP_MAXT>, sp_f64_kernel<D_, P_, R_, SP_MAXT>}
 const SpVariant kSp[] = {
     SPV(8, true, true),  SPV(8, true, false),  SPV(8, false, true),  SPV(8, false, false),
     SPV(16, true, true), SPV(16, true, false), SPV(16, false, true), SPV(16, false, false),
     SPV(32, true, true), SPV(32, true, false), SPV(32, false, true), SPV(32, false, false),
 };
 #undef SPV
+
+bool is_f64(int variant) { return variant == LDPC_F64_SP || variant == LDPC_F64_OMS; }
 }  // namespace
 
 void fill_sp_tables(const ldpc_code& c, int G, SpTables* out) {
@@ -49,7 +52,10 @@ void fill_sp_tables(const ldpc_code& c, int G, SpTables* out) {
 
 int setup_sp(ldpc_ctx* x) {
     const ldpc_code& c = x->code;
-    const bool prod = x->cfg.variant == LDPC_F32_SP;
+    const bool dbl = is_f64(x->cfg.variant);
+    const bool prod = x->cfg.variant == LDPC_F32_SP || x->cfg.variant == LDPC_F64_SP;
+    const size_t es = dbl ? 8 : 4;              // bytes per element
+    const int V = 16 / (int)es;                 // elements per 16 bytes
     if (c.mrow > SP_MAX_L || (int)c.row_cols.size() > SP_MAX_E)
         return fail(LDPC_ERR_UNSUPPORTED, "float decoder: %d layers / %zu edges exceed the tables", c.mrow,
                     c.row_cols.size());
@@ -60,40 +66,54 @@ int setup_sp(ldpc_ctx* x) {
     int G = std::max(1, std::min(32, 128 / c.z));
     if (const char* e = getenv("LDPC_SP_G")) G = std::max(1, std::min(32, atoi(e)));
     while (G > 1 && ((G * c.z + 31) / 32) * 32 > SP_MAXT) --G;
-    fill_sp_tables(c, G, &t);
+    // posteriors + staging of G codewords; fewer codewords per CTA while that
+    // exceeds the shared memory, then no staging buffer
+    const int nstage = (c.z * c.mcol + V - 1) & ~(V - 1);
+    auto base_bytes = [&](int g, bool stage) {
+        fill_sp_tables(c, g, &t);
+        return ((((size_t)g * t.stride + V - 1) & ~(size_t)(V - 1)) + (stage ? (size_t)g * nstage : 0)) * es;
+    };
+    while (G > 1 && base_bytes(G, true) > (size_t)kSpMaxSmem) --G;
+    const bool nostage = base_bytes(G, true) > (size_t)kSpMaxSmem;
+    const size_t base_smem = base_bytes(G, !nostage);   // leaves t filled for G
+    t.nostage = nostage ? 1 : 0;
     x->sp_threads = ((G * c.z + 31) / 32) * 32;
-    const int nstage = (t.n + 3) & ~3;
-    const size_t base_smem = ((((size_t)G * t.stride + 3) & ~(size_t)3) + (size_t)G * nstage) * 4;
-    const size_t r_smem = (size_t)t.E * x->sp_threads * 4;
+    const size_t r_smem = (size_t)t.E * x->sp_threads * es;
     const bool rsmem = base_smem + r_smem <= 160 * 1024;
     const SpVariant* v = nullptr;
     for (const SpVariant& k : kSp)
         if (k.dmax == dmax && k.prod == prod && k.rsmem == rsmem) v = &k;
-    x->sp_kernel = v->k;
+    x->sp_kernel = dbl ? nullptr : v->k;
+    x->sp64_kernel = dbl ? v->k64 : nullptr;
+    const void* kfn = dbl ? (const void*)v->k64 : (const void*)v->k;
     x->sp_smem = (int)(base_smem + (rsmem ? r_smem : 0));
     // up to 220 KB dynamic (B200: 227 KB per CTA, less the kernel's static shared memory)
-    if (x->sp_smem > kSpMaxSmem) return fail(LDPC_ERR_UNSUPPORTED, "float decoder: %d B of shared memory", x->sp_smem);
-    CUDA_TRY(allow_dynamic_smem((const void*)v->k, kSpMaxSmem));
+    if (x->sp_smem > kSpMaxSmem)
+        return fail(LDPC_ERR_UNSUPPORTED, "%s decoder: %d B of shared memory", dbl ? "double" : "float", x->sp_smem);
+    CUDA_TRY(allow_dynamic_smem(kfn, kSpMaxSmem));
     int per_sm = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)v->k, x->sp_threads, x->sp_smem));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, x->sp_threads, x->sp_smem));
     if (per_sm < 1) return fail(LDPC_ERR_UNSUPPORTED, "float decoder: launch does not fit an SM");
     x->sp_ctas = per_sm * x->sms;
     if (!rsmem) {
         CUDA_TRY(cudaMalloc(&x->d_sp_scratch, (size_t)x->sp_ctas * r_smem));
     }
-    // decode_row's Max_row_simd (decode_functions.cpp:27-32) for a float build
-    x->maxf = x->cfg.max_row_metric < 1e-6 ? (float)(1.0 - (double)x->cfg.max_row_metric) : x->cfg.max_row_metric;
+    // decode_row's Max_row_simd (decode_functions.cpp:27-32): 1 - (CTYPE)max_row_metric
+    // below 1e-6 (sum-product), else max_row_metric, in the build's element type
+    const double mrm = (double)x->cfg.max_row_metric;
+    x->maxf = x->cfg.max_row_metric < 1e-6 ? (float)(1.0 - mrm) : x->cfg.max_row_metric;
+    x->maxd = x->cfg.max_row_metric < 1e-6 ? 1.0 - mrm : mrm;
     return LDPC_OK;
 }
 
-int launch_sp(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s) {
-    if (!x->sp_kernel) return fail(LDPC_ERR_INVALID_ARG, "context was not created for a float decoder");
-    if (a.n == 0) return LDPC_OK;
-    SpJob job;
+namespace {
+template <class T>
+SpJobT<T> sp_job(const ldpc_ctx* x, const DecodeArgs& a, T maxv) {
+    SpJobT<T> job;
     memset(&job, 0, sizeof(job));
-    job.llr = (const float*)a.llr;
+    job.llr = (const T*)a.llr;
     job.ncw = (long long)a.n;
-    job.post_out = (float*)a.post;
+    job.post_out = (T*)a.post;
     job.hard_out = a.hard;
     job.iters_out = a.iters;
     job.ref_bits = a.ref_bits;
@@ -103,13 +123,23 @@ int launch_sp(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s) {
     job.n_buckets = std::max(1, std::min(a.n_buckets, OMS_MAX_BUCKETS));
     job.num_par = x->code.num_par;
     job.max_iter = (int)x->cfg.max_iter;
-    job.prod = x->cfg.variant == LDPC_F32_SP;
-    job.beta = x->cfg.beta;
-    job.maxv = x->maxf;
-    job.r_scratch = x->d_sp_scratch;
+    job.prod = x->cfg.variant == LDPC_F32_SP || x->cfg.variant == LDPC_F64_SP;
+    job.beta = (T)x->cfg.beta;
+    job.maxv = maxv;
+    job.r_scratch = (T*)x->d_sp_scratch;
+    return job;
+}
+}  // namespace
+
+int launch_sp(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s) {
+    if (!x->sp_kernel && !x->sp64_kernel) return fail(LDPC_ERR_INVALID_ARG, "context was not created for a float decoder");
+    if (a.n == 0) return LDPC_OK;
     const long long want = ((long long)a.n + x->spt.G - 1) / x->spt.G;
     const int grid = (int)std::min<long long>(want, x->sp_ctas);
-    x->sp_kernel<<<grid, x->sp_threads, x->sp_smem, s>>>(x->spt, job);
+    if (x->sp64_kernel)
+        x->sp64_kernel<<<grid, x->sp_threads, x->sp_smem, s>>>(x->spt, sp_job<double>(x, a, x->maxd));
+    else
+        x->sp_kernel<<<grid, x->sp_threads, x->sp_smem, s>>>(x->spt, sp_job<float>(x, a, x->maxf));
     CUDA_TRY(cudaGetLastError());
     return LDPC_OK;
 }

@@ -96,6 +96,7 @@ int launch_gen(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* snr_
     // integer LLRs of the context's element type
     if (x->cfg.variant == LDPC_INT16_OMS) job.llr_i16 = (int16_t*)llr_int;
     else if (x->cfg.variant == LDPC_INT32_OMS) job.llr_i32 = (int32_t*)llr_int;
+    else if (x->cfg.variant == LDPC_F64_SP || x->cfg.variant == LDPC_F64_OMS) job.llr_f64 = (double*)llr_int;
     else job.llr_i8 = (int8_t*)llr_int;
     job.llr_f32 = llr_f32;
     job.data_bits = data_bits;

@@ -230,6 +230,9 @@ __global__ void __launch_bounds__(256) gen_kernel(const __grid_constant__ GenTab
                         if (job.llr_i32) job.llr_i32[row * tb.n + idx0 + q] = v;
                     }
                 }
+                if (job.llr_f64) {
+                    for (int q = 0; q < 4 && idx0 + q < tb.n; ++q) job.llr_f64[row * tb.n + idx0 + q] = (double)l[q];
+                }
                 if (job.llr_f32) {
                     float* dst = job.llr_f32 + row * tb.n + idx0;
                     if ((tb.n & 3) == 0) {
@@ -293,6 +296,7 @@ __global__ void llr_from_noise_kernel(const GenTables tb, const uint8_t* bits, c
         if (out_int) {
             if (int_bytes == 1) static_cast<int8_t*>(out_int)[e] = llr_to_i8(l);
             else if (int_bytes == 2) static_cast<int16_t*>(out_int)[e] = (int16_t)__float2int_rn(l);
+            else if (int_bytes == 8) static_cast<double*>(out_int)[e] = (double)l;
             else static_cast<int32_t*>(out_int)[e] = __float2int_rn(l);
         }
         if (out_f32) out_f32[e] = l;

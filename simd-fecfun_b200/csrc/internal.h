@@ -21,6 +21,7 @@ int fail(int code, const char* fmt, ...);
 
 typedef void (*oms_fn)(const OmsTables, const OmsJob);
 typedef void (*sp_fn)(const SpTables, const SpJob);
+typedef void (*sp64_fn)(const SpTables, const SpJobT<double>);
 typedef void (*rt_fn)(const RtLaunch);
 
 // The dynamic shared-memory limit is an attribute of the kernel function,
@@ -107,9 +108,11 @@ struct ldpc_ctx {
     // float decoders
     ldpc::SpTables spt;
     ldpc::sp_fn sp_kernel = nullptr;
+    ldpc::sp64_fn sp64_kernel = nullptr;        // double variants
     int sp_threads = 0, sp_smem = 0, sp_ctas = 0;
     float* d_sp_scratch = nullptr;              // check messages of large codes (global)
     float maxf = 0.f;
+    double maxd = 0.0;                          // Max_val of the double variants
     // int16 / int32 decoders (tables in spt)
     void* int_kernel = nullptr;
     int int_threads = 0, int_smem = 0, int_ctas = 0;
@@ -158,7 +161,8 @@ int launch_int(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s);
 int launch_decode(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s);
 // bytes per LLR / posterior element of a variant
 inline int llr_bytes(int variant) {
-    return variant == LDPC_INT8_OMS ? 1 : variant == LDPC_INT16_OMS ? 2 : 4;
+    return variant == LDPC_INT8_OMS ? 1 : variant == LDPC_INT16_OMS ? 2
+           : (variant == LDPC_F64_SP || variant == LDPC_F64_OMS) ? 8 : 4;
 }
 int setup_sp(ldpc_ctx* x);
 // float-decoder tables of a code for G codewords per CTA

@@ -1,6 +1,7 @@
-// Layered float32 decoders: sum-product (tanh / product tree / 2 atanh) and
-// offset min-sum, bit-exact with the reference's SIMD_ELEM_BW=-32 builds
-// (LDPCtop_Vec16f_prod, LDPCtop_Vec16f_min):
+// Layered float decoders: sum-product (tanh / product tree / 2 atanh) and
+// offset min-sum, in float (bit-exact with the reference's SIMD_ELEM_BW=-32
+// builds LDPCtop_Vec16f_prod / Vec16f_min) and in double (the SIMD_ELEM_BW=-64
+// builds LDPCtop_Vec8d_prod / Vec8d_min):
 //   Q = P - R                                  decode_functions.cpp:53
 //   a = max(|Q| - beta, 0)                     :56-62
 //   x = tanh(a/2) (sum-product) or a           min_find.pl:37-41
@@ -8,7 +9,7 @@
 //         clamped at Max_val, then 2 atanh(.)  min_find.pl:99-107, 44-45
 //   R' = f_j with the sign of prod_{k!=j} Q_k  decode_functions.cpp:85-87
 //   P  = Q + R'                                :91
-// with the same float operations in the same order as the oracle (no fused
+// with the same operations in the same order as the oracle (no fused
 // multiply-adds; tanh/atanh from ldpc_math.h), so posteriors agree bit for bit.
 //
 // Work layout: G codewords per CTA, one per group of Z threads (thread
@@ -16,7 +17,10 @@
 // messages in shared memory (RSMEM) or, for large codes, in a global scratch
 // area; the layer loop runs over run-time tables, so any code shape works.
 // The iteration boundary (syndrome, write-out, refill from a prefetched
-// staging buffer) follows the int8 kernel.
+// staging buffer) follows the int8 kernel.  Codes whose posteriors and
+// staging do not both fit shared memory (double, 5G NR base graph 1 at large
+// Z) run without the staging buffer (tb.nostage): a finished codeword's slot
+// is refilled straight from global memory.
 #pragma once
 #include <stdint.h>
 
@@ -37,22 +41,56 @@ __device__ __forceinline__ void sp_cp_async4(void* smem, const void* gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
 }
 
-__device__ __forceinline__ void sp_prefetch(float* stage, const float* llr, long long cw, int n, int lane) {
-    const float* src = llr + cw * (long long)n;
+__device__ __forceinline__ void sp_cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+
+// element operations of the float and double decoders: IEEE round to nearest,
+// never contracted into fused multiply-adds
+__device__ __forceinline__ float sp_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sp_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float sp_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double sp_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float sp_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double sp_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float sp_abs(float a) { return fabsf(a); }
+__device__ __forceinline__ double sp_abs(double a) { return fabs(a); }
+__device__ __forceinline__ float sp_tanh(float a) { return lm_tanh(a); }
+__device__ __forceinline__ double sp_tanh(double a) { return lmd_tanh(a); }
+__device__ __forceinline__ float sp_atanh(float a) { return lm_atanh(a); }
+__device__ __forceinline__ double sp_atanh(double a) { return lmd_atanh(a); }
+// the 32-bit word that holds the sign (bit 31)
+__device__ __forceinline__ uint32_t sp_signw(float v) { return __float_as_uint(v); }
+__device__ __forceinline__ uint32_t sp_signw(double v) { return (uint32_t)__double2hiint(v); }
+// v with its sign flipped where bit 31 of sg is set (sign_combine)
+__device__ __forceinline__ float sp_flip(float v, uint32_t sg) { return __uint_as_float(__float_as_uint(v) ^ sg); }
+__device__ __forceinline__ double sp_flip(double v, uint32_t sg) {
+    return __hiloint2double(__double2hiint(v) ^ (int)sg, __double2loint(v));
+}
+
+template <class T>
+__device__ __forceinline__ void sp_prefetch(T* stage, const T* llr, long long cw, int n, int lane) {
+    constexpr int V = 16 / (int)sizeof(T);   // elements per 16-byte copy
+    const T* src = llr + cw * (long long)n;
     const unsigned long long base = reinterpret_cast<unsigned long long>(src);
-    if ((n & 3) == 0 && (base & 15) == 0) {
-        for (int i = 4 * lane; i < n; i += 128) sp_cp_async16(stage + i, src + i);
+    if ((n % V) == 0 && (base & 15) == 0) {
+        for (int i = V * lane; i < n; i += 32 * V) sp_cp_async16(stage + i, src + i);
+    } else if (sizeof(T) == 8) {
+        for (int i = lane; i < n; i += 32) sp_cp_async8(stage + i, src + i);
     } else {
         for (int i = lane; i < n; i += 32) sp_cp_async4(stage + i, src + i);
     }
 }
 
 // Decode codewords [lo, hi) of job with the CTA: the whole decoder; sm_f is
-// the CTA's dynamic shared memory for posteriors, staging and (RSMEM)
-// messages, r_cta its global message area otherwise.
-template <int DMAX, bool PROD, bool RSMEM>
-__device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJob& job, long long lo, long long hi,
-                                                float* sm_f, float* r_cta) {
+// the CTA's dynamic shared memory (16-byte aligned) for posteriors, staging
+// and (RSMEM) messages, r_cta its global message area otherwise.  T = float
+// or double.
+template <int DMAX, bool PROD, bool RSMEM, class T>
+__device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJobT<T>& job, long long lo, long long hi,
+                                                T* sm_f, T* r_cta) {
+    constexpr int V = 16 / (int)sizeof(T);
     __shared__ long long s_cur[32];
     __shared__ long long s_next[32];
     __shared__ int s_it[32];
@@ -68,16 +106,17 @@ __device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJob&
     const int t = tid / G, g = tid - (tid / G) * G;
     const bool active = t < z;
     const int gbase = g * stride;
-    float* Ps = sm_f;
-    float* stage = sm_f + ((G * stride + 3) & ~3);                  // [G][nstage], 16-byte aligned
-    const int nstage = (n + 3) & ~3;
-    float* Rbase = RSMEM ? stage + G * nstage : r_cta;
-    float* Rt = Rbase + tid;                                        // message of edge e at Rt[e * nthr]
-    const float beta = job.beta, maxv = job.maxv;
+    const bool staged = !tb.nostage;
+    T* Ps = sm_f;
+    T* stage = sm_f + ((G * stride + V - 1) & ~(V - 1));            // [G][nstage], 16-byte aligned
+    const int nstage = (n + V - 1) & ~(V - 1);
+    T* Rbase = RSMEM ? stage + (staged ? G * nstage : 0) : r_cta;
+    T* Rt = Rbase + tid;                                            // message of edge e at Rt[e * nthr]
+    const T beta = job.beta, maxv = job.maxv;
 
     for (int i = tid; i < OMS_MAX_BUCKETS * 4; i += nthr) (&s_cnt[0][0])[i] = 0;
-    for (int i = tid; i < G * stride; i += nthr) Ps[i] = 0.f;
-    for (int e = 0; e < tb.E; ++e) Rt[e * nthr] = 0.f;
+    for (int i = tid; i < G * stride; i += nthr) Ps[i] = T(0);
+    for (int e = 0; e < tb.E; ++e) Rt[e * nthr] = T(0);
     if (tid < 32) {
         const long long c0 = lo + tid, c1 = lo + G + tid;
         s_cur[tid] = tid < G && c0 < hi ? c0 : -1;
@@ -89,23 +128,23 @@ __device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJob&
     __syncthreads();
     for (int k = warp; k < G; k += nwarps) {
         if (s_cur[k] >= 0) {
-            const float* src = job.llr + s_cur[k] * (long long)n;
+            const T* src = job.llr + s_cur[k] * (long long)n;
             for (int i = lane; i < n; i += 32) Ps[k * stride + i] = src[i];
         }
-        if (s_next[k] >= 0) sp_prefetch(stage + k * nstage, job.llr, s_next[k], n, lane);
+        if (staged && s_next[k] >= 0) sp_prefetch(stage + k * nstage, job.llr, s_next[k], n, lane);
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
     __syncthreads();
 
-    auto comb = [](float a, float b) { return PROD ? __fmul_rn(a, b) : (a < b ? a : b); };
-    auto clampf = [maxv](float v) { return maxv < v ? maxv : v; };
+    auto comb = [](T a, T b) { return PROD ? sp_mul(a, b) : (a < b ? a : b); };
+    auto clampf = [maxv](T v) { return maxv < v ? maxv : v; };
 
     for (int par = 0;; par ^= 1) {
         // ================= one layered iteration =================
         for (int l = 0; l < tb.L; ++l) {
             if (active) {
                 const int d = tb.rw[l], eb = tb.ebase[l];
-                float q[DMAX], x[DMAX], f[DMAX];
+                T q[DMAX], x[DMAX], f[DMAX];
                 int addr[DMAX];
                 uint32_t rx = 0;
 #pragma unroll
@@ -113,22 +152,22 @@ __device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJob&
                     if (j < d) {
                         const int e = eb + j;
                         addr[j] = gbase + tb.colz[e] + sp_wrap(t, tb.shift[e], z);
-                        const float Q = __fsub_rn(Ps[addr[j]], Rt[e * nthr]);
+                        const T Q = sp_sub(Ps[addr[j]], Rt[e * nthr]);
                         q[j] = Q;
-                        float a = __fsub_rn(fabsf(Q), beta);
-                        a = a > 0.0f ? a : 0.0f;
-                        x[j] = PROD ? lm_tanh(__fmul_rn(a, 0.5f)) : a;
-                        rx ^= __float_as_uint(Q);
+                        T a = sp_sub(sp_abs(Q), beta);
+                        a = a > T(0) ? a : T(0);
+                        x[j] = PROD ? sp_tanh(sp_mul(a, T(0.5))) : a;
+                        rx ^= sp_signw(Q);
                     }
                 }
                 run_tree<DMAX>(d, x, f, comb, clampf);
 #pragma unroll
                 for (int j = 0; j < DMAX; ++j) {
                     if (j < d) {
-                        const float fj = PROD ? __fmul_rn(2.0f, lm_atanh(f[j])) : f[j];
-                        const uint32_t sg = (rx ^ __float_as_uint(q[j])) & 0x80000000u;
-                        const float rn = __uint_as_float(__float_as_uint(fj) ^ sg);
-                        Ps[addr[j]] = __fadd_rn(q[j], rn);
+                        const T fj = PROD ? sp_mul(T(2), sp_atanh(f[j])) : f[j];
+                        const uint32_t sg = (rx ^ sp_signw(q[j])) & 0x80000000u;
+                        const T rn = sp_flip(fj, sg);
+                        Ps[addr[j]] = sp_add(q[j], rn);
                         Rt[(eb + j) * nthr] = rn;
                     }
                 }
@@ -145,7 +184,7 @@ __device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJob&
                 uint32_t xr = 0;
                 for (int j = 0; j < d; ++j) {
                     const int e = eb + j;
-                    xr ^= __float_as_uint(Ps[gbase + tb.colz[e] + sp_wrap(t, tb.shift[e], z)]);
+                    xr ^= sp_signw(Ps[gbase + tb.colz[e] + sp_wrap(t, tb.shift[e], z)]);
                 }
                 if (xr & 0x80000000u) {
                     atomicOr(&s_synd[par], 1u << g);
@@ -167,7 +206,7 @@ __device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJob&
                 if (lane == 0) { s_it[k] = it; s_busy[par] = 1; }
                 continue;
             }
-            const float* pk = Ps + k * stride;
+            const T* pk = Ps + k * stride;
             const uint32_t* ref = job.ref_bits ? job.ref_bits + (cw % job.ref_period) * tb.hard_words : nullptr;
             uint32_t mine = 0, refw = 0, errw = 0;
             unsigned errslots = 0;
@@ -176,7 +215,7 @@ __device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJob&
                 const int wn = min(32, tb.hard_words - w0);
                 for (int w = 0; w < wn; ++w) {
                     const int i = (w0 + w) * 32 + lane;
-                    const bool b = (i < tb.kbits) && (pk[i] < 0.0f);
+                    const bool b = (i < tb.kbits) && (pk[i] < T(0));
                     const uint32_t word = __ballot_sync(0xffffffffu, b);
                     if (lane == w) mine = word;
                     if (ref) {
@@ -189,7 +228,7 @@ __device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJob&
                 if (job.hard_out && lane < wn) job.hard_out[cw * tb.hard_words + w0 + lane] = mine;
             }
             if (job.post_out) {
-                float* dst = job.post_out + cw * (long long)n;
+                T* dst = job.post_out + cw * (long long)n;
                 for (int i = lane; i < n; i += 32) dst[i] = pk[i];
             }
             if (lane == 0 && job.iters_out) job.iters_out[cw] = (uint8_t)it;
@@ -209,14 +248,14 @@ __device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJob&
             __syncwarp();
             const long long nxt = s_next[k];
             if (nxt >= 0) {
-                const float* st = stage + k * nstage;
+                const T* st = staged ? stage + k * nstage : job.llr + nxt * (long long)n;
                 for (int i = lane; i < n; i += 32) Ps[k * stride + i] = st[i];
                 __syncwarp();
                 unsigned long long c = 0;
                 if (lane == 0) c = atomicAdd(&s_head, 1ull);
                 c = __shfl_sync(0xffffffffu, c, 0);
                 const long long fresh = (long long)c < hi ? (long long)c : -1;
-                if (fresh >= 0) sp_prefetch(stage + k * nstage, job.llr, fresh, n, lane);
+                if (staged && fresh >= 0) sp_prefetch(stage + k * nstage, job.llr, fresh, n, lane);
                 if (lane == 0) { s_next[k] = fresh; s_busy[par] = 1; }
             }
             if (lane == 0) {
@@ -228,7 +267,7 @@ __device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJob&
         asm volatile("cp.async.commit_group;" ::: "memory");
         __syncthreads();
         if (active && (s_zero[par] & (1u << g)))
-            for (int e = 0; e < tb.E; ++e) Rt[e * nthr] = 0.f;
+            for (int e = 0; e < tb.E; ++e) Rt[e * nthr] = T(0);
         if (!s_busy[par]) break;
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
@@ -243,9 +282,18 @@ __device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJob&
 
 template <int DMAX, bool PROD, bool RSMEM, int MAXT>
 __global__ void __launch_bounds__(MAXT) sp_f32_kernel(const __grid_constant__ SpTables tb, const __grid_constant__ SpJob job) {
-    extern __shared__ float sm_f[];
+    extern __shared__ __align__(16) float sm_f[];
     const long long lo = job.ncw * blockIdx.x / gridDim.x, hi = job.ncw * (blockIdx.x + 1) / gridDim.x;
     sp_decode_range<DMAX, PROD, RSMEM>(tb, job, lo, hi, sm_f,
+                                       RSMEM ? nullptr : job.r_scratch + (long long)blockIdx.x * tb.E * blockDim.x);
+}
+
+template <int DMAX, bool PROD, bool RSMEM, int MAXT>
+__global__ void __launch_bounds__(MAXT) sp_f64_kernel(const __grid_constant__ SpTables tb,
+                                                      const __grid_constant__ SpJobT<double> job) {
+    extern __shared__ __align__(16) double sm_d[];
+    const long long lo = job.ncw * blockIdx.x / gridDim.x, hi = job.ncw * (blockIdx.x + 1) / gridDim.x;
+    sp_decode_range<DMAX, PROD, RSMEM>(tb, job, lo, hi, sm_d,
                                        RSMEM ? nullptr : job.r_scratch + (long long)blockIdx.x * tb.E * blockDim.x);
 }
 

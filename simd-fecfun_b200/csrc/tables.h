@@ -47,16 +47,18 @@ struct SpTables {
     int stride;                      // posterior words per group in shared memory
     int kbits, hard_words;
     int E;                           // sum of row weights
+    int nostage;                     // 1: no shared staging buffer; refill from global memory
     int16_t rw[SP_MAX_L];
     int16_t ebase[SP_MAX_L];         // first edge of layer l
     int32_t colz[SP_MAX_E];          // column * Z of edge e
     int16_t shift[SP_MAX_E];
 };
 
-struct SpJob {
-    const float* llr;
+template <class T>                   // T = float or double
+struct SpJobT {
+    const T* llr;
     long long ncw;
-    float* post_out;
+    T* post_out;
     uint32_t* hard_out;
     uint8_t* iters_out;
     const uint32_t* ref_bits;
@@ -67,10 +69,11 @@ struct SpJob {
     int num_par;
     int max_iter;
     int prod;                        // 1 = sum-product, 0 = offset min-sum
-    float beta;
-    float maxv;                      // Max_val as decode_row computes it
-    float* r_scratch;                // global check messages when they do not fit shared memory
+    T beta;
+    T maxv;                          // Max_val as decode_row computes it
+    T* r_scratch;                    // global check messages when they do not fit shared memory
 };
+using SpJob = SpJobT<float>;
 
 // ---- int8 offset min-sum with run-time code tables (any shape; several codes per launch) ----
 constexpr int RT_MAX_L = 64;
@@ -154,6 +157,7 @@ struct GenJob {
     int8_t* llr_i8;                  // [n_snr][n_per_snr][n] or null
     int16_t* llr_i16;                // int16 contexts (gen_metrics: roundi, then compress)
     int32_t* llr_i32;                // int32 contexts (gen_metrics: roundi)
+    double* llr_f64;                 // double contexts (gen_metrics: to_double of the float LLR)
     float* llr_f32;                  // [n_snr][n_per_snr][n] or null
     uint32_t* data_bits;             // [n_per_snr][hard_words] or null
     unsigned long long* uncoded;     // [n_snr] or null

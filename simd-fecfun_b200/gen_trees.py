@@ -2,9 +2,9 @@
 update (ldpc_b200/trees.py, the schedule of the reference's min_find.pl) as
 straight-line device code, one function per row weight.
 
-    tree_<d>(float* x, float maxv, float* out)   x: inputs, overwritten as nodes
+    tree_<d>(T* x, T* out, comb, clamp)   T = float or double
 
-with COMB(a, b) and CLAMP(v) supplied by the including kernel.  Run by
+with comb(a, b) and clamp(v) supplied by the including kernel.  Run by
 build.py before compiling; the output is a build product (git-ignored).
 """
 import os
@@ -23,9 +23,9 @@ def generate(path):
     for d in range(2, MAX_D + 1):
         ops, outs, masks = trees.tree_program(d)
         nn = len(masks)
-        out.append("template <class Comb, class Clamp>")
-        out.append("__device__ __forceinline__ void tree_%d(float* x, float* out, Comb comb, Clamp clamp) {" % d)
-        out.append("    float n[%d];" % nn)
+        out.append("template <class T, class Comb, class Clamp>")
+        out.append("__device__ __forceinline__ void tree_%d(T* x, T* out, Comb comb, Clamp clamp) {" % d)
+        out.append("    T n[%d];" % nn)
         out.append("#pragma unroll")
         out.append("    for (int i = 0; i < %d; ++i) n[i] = x[i];" % d)
         for op in ops:
@@ -37,8 +37,8 @@ def generate(path):
             out.append("    out[%d] = n[%d];" % (j, k))
         out.append("}")
         out.append("")
-    out.append("template <int DMAX, class Comb, class Clamp>")
-    out.append("__device__ __forceinline__ void run_tree(int d, float* x, float* out, Comb comb, Clamp clamp) {")
+    out.append("template <int DMAX, class T, class Comb, class Clamp>")
+    out.append("__device__ __forceinline__ void run_tree(int d, T* x, T* out, Comb comb, Clamp clamp) {")
     out.append("    switch (d) {")
     for d in range(2, MAX_D + 1):
         out.append("        case %d: if constexpr (DMAX >= %d) tree_%d(x, out, comb, clamp); break;" % (d, d, d))

@@ -29,6 +29,8 @@ LDPC_F32_SP = 1
 LDPC_F32_OMS = 2
 LDPC_INT16_OMS = 3
 LDPC_INT32_OMS = 4
+LDPC_F64_SP = 5
+LDPC_F64_OMS = 6
 
 ERROR_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "BAD_TABLE", 3: "UNSUPPORTED", 4: "CUDA", 5: "TIMEOUT", 6: "IO",
                7: "NOMEM"}
@@ -79,6 +81,8 @@ _PROTOS = {
     "ldpc_decode_f32": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _vp]),
     "ldpc_decode_int16": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _vp]),
     "ldpc_decode_int32": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _vp]),
+    "ldpc_decode_f64": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _vp]),
+    "ldpc_decode_f64_host": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, C.POINTER(C.c_uint64)]),
     "ldpc_decode_int16_host": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, C.POINTER(C.c_uint64)]),
     "ldpc_decode_int32_host": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, C.POINTER(C.c_uint64)]),
     "ldpc_decode_int8_host": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, C.POINTER(C.c_uint64)]),
@@ -236,6 +240,9 @@ class Context:
     def decode_int32(self, llr, n, post=None, hard=None, iters=None, stream=0):
         check(lib.ldpc_decode_int32(self.h, _ptr(llr), n, _ptr(post), _ptr(hard), _ptr(iters), stream or None))
 
+    def decode_f64(self, llr, n, post=None, hard=None, iters=None, stream=0):
+        check(lib.ldpc_decode_f64(self.h, _ptr(llr), n, _ptr(post), _ptr(hard), _ptr(iters), stream or None))
+
     def decode_count(self, llr, n, hard=None, iters=None, data_bits=None, ref_period=1, bucket_size=0, counters=None,
                      n_buckets=1, stream=0):
         check(lib.ldpc_decode_count(self.h, _ptr(llr), n, _ptr(hard), _ptr(iters), _ptr(data_bits), ref_period,
@@ -243,7 +250,8 @@ class Context:
 
     def generate(self, seed, cw_offset, snr_db, n_per_snr, llr_i8=None, llr_f32=None, data_bits=None, uncoded=None,
                  stream=0, llr_int=None):
-        """llr_int (alias llr_i8): integer LLRs of the context's element type."""
+        """llr_int (alias llr_i8): LLRs of the context's element type (int8,
+        int16, int32, or double for the double variants)."""
         llr_i8 = llr_int if llr_int is not None else llr_i8
         snr = np.ascontiguousarray(snr_db, dtype=np.float32)
         check(lib.ldpc_generate(self.h, seed, cw_offset, snr.ctypes.data, snr.size, n_per_snr, _ptr(llr_i8),
@@ -280,7 +288,8 @@ class Context:
         iters = np.empty(n, np.uint8) if want_iters else None
         tot = C.c_uint64()
         fns = {np.dtype(np.int8): lib.ldpc_decode_int8_host, np.dtype(np.float32): lib.ldpc_decode_f32_host,
-               np.dtype(np.int16): lib.ldpc_decode_int16_host, np.dtype(np.int32): lib.ldpc_decode_int32_host}
+               np.dtype(np.int16): lib.ldpc_decode_int16_host, np.dtype(np.int32): lib.ldpc_decode_int32_host,
+               np.dtype(np.float64): lib.ldpc_decode_f64_host}
         if llr.dtype not in fns:
             raise TypeError(llr.dtype)
         fn = fns[llr.dtype]

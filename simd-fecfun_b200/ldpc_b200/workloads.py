@@ -16,6 +16,10 @@
   vs plain offsets.
 * :func:`sp_sweep` -- float sum-product on 802.16e 1/2 for all 19 lifting
   sizes Z = 24..96.
+* :func:`variants` -- the headline 802.11ad 1/2 simulation point decoded by
+  every decoder variant of the reference's LDPCtop family (int8/int16/int32
+  offset min-sum, float and double offset min-sum and sum-product), each
+  with the Perl driver's parameters for that variant.
 
 Inputs are synthetic, drawn on the device by the library's generator
 (Philox data bits, QC encoding, AWGN); SNRs given as Eb/N0 are converted to
@@ -366,3 +370,44 @@ def sp_sweep(cw_per_z: int = 1 << 20, ebn0=(0.5, 1.0, 1.5, 2.0), seed: int = 5, 
         "gpu_launches": steps,
         "quality": quality,
     }
+
+
+# (label, variant, reference build, max_row_metric, beta, LLR scale, max |LLR|):
+# the Perl driver's defaults (run_LDPCsim.pl:29-32), and for sum-product its
+# overrides (run_LDPCsim.pl:56-63: clamp 1-6e-8 float, 1-1e-16 double)
+VARIANT_RUNS = [
+    ("int8 offset min-sum", capi.LDPC_INT8_OMS, "Vec64c_min", 31.0, 1.0, 2.0, 24.0),
+    ("int16 offset min-sum", capi.LDPC_INT16_OMS, "Vec32s_min", 31.0, 1.0, 2.0, 24.0),
+    ("int32 offset min-sum", capi.LDPC_INT32_OMS, "Vec16w_min", 31.0, 1.0, 2.0, 24.0),
+    ("float offset min-sum", capi.LDPC_F32_OMS, "Vec16f_min", 31.0, 1.0, 2.0, 24.0),
+    ("float sum-product", capi.LDPC_F32_SP, "Vec16f_prod", 6e-8, 0.0, 1.0, 1e9),
+    ("double offset min-sum", capi.LDPC_F64_OMS, "Vec8d_min", 31.0, 1.0, 2.0, 24.0),
+    ("double sum-product", capi.LDPC_F64_SP, "Vec8d_prod", 1e-16, 0.0, 1.0, 1e9),
+]
+
+
+def variants(n_per_snr: int = 200_000, snrs=(-1.0, -0.75, -0.5, -0.25, 0.0), seed: int = 17,
+             max_iter: int = 10) -> List[Dict]:
+    """802.11ad 1/2 at the headline SNR points through ldpc_simulate for each
+    variant: the generator writes LLRs of the variant's element type, the
+    decoder runs with fused counting, and only the decoder's device time
+    (CUDA events around each launch) counts.  One untimed pass first."""
+    code = codes.make_code("11ad 1/2")
+    h = capi.Code.from_tables(code)
+    out = []
+    for label, variant, ref, mrm, beta, scale, max_abs in VARIANT_RUNS:
+        ctx = capi.Context(h, variant=variant, max_iter=max_iter, max_row_metric=mrm, beta=beta, llr_scale=scale,
+                           max_abs_llr=max_abs)
+        ctx.simulate(seed=seed, cw_offset=1 << 40, snr_db=list(snrs), n_per_snr=min(n_per_snr, 20_000))
+        st = ctx.simulate(seed=seed, cw_offset=0, snr_db=list(snrs), n_per_snr=n_per_snr)
+        cw = sum(x["codewords"] for x in st)
+        ms = sum(x["decode_ms"] for x in st)
+        out.append({
+            "variant": label, "reference_build": "LDPCtop_" + ref, "codewords": cw, "decode_ms": ms,
+            "value": cw / (ms * 1e-3), "unit": "codewords/s",
+            "params": {"max_row_metric": mrm, "beta": beta, "llr_scale": scale, "max_abs_llr": max_abs},
+            "avg_iter": sum(x["iterations"] for x in st) / cw,
+            "quality": [{"snr_db": x["snr_db"], "cwer": x["cw_errors"] / x["codewords"],
+                         "ber": x["bit_errors"] / (x["codewords"] * code.k)} for x in st],
+        })
+    return out

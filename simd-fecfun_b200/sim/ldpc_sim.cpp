@@ -15,7 +15,8 @@
 //
 // The decoder variant comes from the program name, as the Perl driver reads
 // it (run_LDPCsim.pl:51-66): Vec<n>c / s / w -> int8 / int16 / int32 offset
-// min-sum, Vec<n>f -> float offset min-sum, or sum-product with "_prod".
+// min-sum, Vec<n>f / d -> float / double offset min-sum, or sum-product with
+// "_prod".
 //
 // Differences from the reference, by design:
 //   - noise and data come from Philox4x32-10 keyed by one 64-bit value that
@@ -102,7 +103,7 @@ int variant_from_name(const char* argv0) {
         case 's': return LDPC_INT16_OMS;
         case 'w': return LDPC_INT32_OMS;
         case 'f': return prod ? LDPC_F32_SP : LDPC_F32_OMS;
-        case 'd': return -1;
+        case 'd': return prod ? LDPC_F64_SP : LDPC_F64_OMS;
         default: return prod ? -1 : LDPC_INT8_OMS;
     }
 }
@@ -138,7 +139,7 @@ int main(int argc, char** argv) {
     ldpc_cfg cfg;
     cfg.variant = variant_from_name(argv[0]);
     if (cfg.variant < 0) {
-        printf("ERROR: decoder variant of %s is not built (double, or sum-product on integers)\n", argv[0]);
+        printf("ERROR: decoder variant of %s is not built (sum-product on integers)\n", argv[0]);
         return 1;
     }
     cfg.max_iter = sim.max_iter;

@@ -1,7 +1,7 @@
 """Golden vectors from the reference's own code (oracle/_ref build).
 
 Runs the reference's decoders (LDPCdecode_set, int8 min-sum / float
-sum-product / float min-sum), encoder (LDPCencode) and LLR generator
+and double sum-product / float and double min-sum), encoder (LDPCencode) and LLR generator
 (gen_metrics) -- all built from its unmodified sources by
 ``make -C oracle ref`` -- on seeded inputs and stores inputs and outputs in
 ``ref_vectors.npz``.  The CPU tests check the oracle against these without
@@ -60,6 +60,19 @@ def main():
         lib = rb.RefLib(variant)
         for ctag, name, snr, n in (("11ad", "11ad 1/2", -0.5, 16), ("16e", "16e 1/2", 1.0, 8)):
             code = codes.make_code(name, elem_size=32)
+            ctx, wgn, unc = ref_pipeline(lib, code, n, snr, 1.0, 1e9, 9)
+            llr = ctx.posteriors()
+            it = ctx.decode_each(10, mrm, beta)
+            out["%s_%s_llr" % (tag, ctag)] = llr
+            out["%s_%s_post" % (tag, ctag)] = ctx.posteriors()
+            out["%s_%s_iters" % (tag, ctag)] = it
+    # double sum-product (the Perl driver's clamp for d_prod, run_LDPCsim.pl:59)
+    # and double min-sum (8-lane tables); gen_metrics widens the float LLRs to
+    # double (gen_metrics.cpp:91-93)
+    for variant, tag, mode, mrm, beta in (("Vec8d_prod", "f64sp", 1, 1e-16, 0.0), ("Vec8d_min", "f64ms", 0, 31.0, 0.5)):
+        lib = rb.RefLib(variant)
+        for ctag, name, snr, n in (("11ad", "11ad 1/2", -0.5, 16), ("16e", "16e 1/2", 1.0, 8)):
+            code = codes.make_code(name, elem_size=64)
             ctx, wgn, unc = ref_pipeline(lib, code, n, snr, 1.0, 1e9, 9)
             llr = ctx.posteriors()
             it = ctx.decode_each(10, mrm, beta)

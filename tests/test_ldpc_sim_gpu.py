@@ -1,7 +1,7 @@
 """ldpc_sim on the GPU: the lines it prints for the reference's stdin blob
 carry exactly the counters of ldpc_simulate with the same generator key and
 codeword offsets (one outer loop = loop_count * num_codeword codewords per
-SNR point), for the int8 and the float sum-product variants."""
+SNR point), for the int8, int16, float and double sum-product variants."""
 import os
 import subprocess
 
@@ -18,6 +18,7 @@ SIM = os.path.join(ROOT, "simd-fecfun_b200", "ldpc_b200", "ldpc_sim")
     ("LDPCtop_Vec64c_min_b200", "11ad 1/2", dict(mrm=31.0, scale=2.0, max_abs=24.0, beta=1.0, snr=(-1.0, 0.0, 0.5))),
     ("LDPCtop_Vec16f_prod_b200", "16e 1/2", dict(mrm=6e-8, scale=1.0, max_abs=1e9, beta=0.0, snr=(0.5, 1.5, 0.5))),
     ("LDPCtop_Vec32s_min_b200", "11n 1/2 z27", dict(mrm=400.0, scale=20.0, max_abs=800.0, beta=5.0, snr=(0.5, 1.5, 1.0))),
+    ("LDPCtop_Vec8d_prod_b200", "11ad 1/2", dict(mrm=1e-16, scale=1.0, max_abs=1e9, beta=0.0, snr=(-0.5, 0.5, 1.0))),
 ])
 def test_lines_match_simulate(capi, tmp_path, exe, name, params):
     from ldpc_b200 import codes
@@ -35,7 +36,8 @@ def test_lines_match_simulate(capi, tmp_path, exe, name, params):
     assert out["cw_count"] == inner * ncw and out["matrix"][:3] == (code.z, code.mcol, code.mrow)
     snrs = [s0 + k * st for k in range(int((s1 - s0 + 1e-6) / st) + 1)]
     assert len(out["loops"]) == outer * len(snrs)
-    variant = {"64c": capi.LDPC_INT8_OMS, "32s": capi.LDPC_INT16_OMS}.get(exe[11:14], capi.LDPC_F32_SP)
+    variant = {"64c": capi.LDPC_INT8_OMS, "32s": capi.LDPC_INT16_OMS, "8d_": capi.LDPC_F64_SP}.get(exe[11:14],
+                                                                                             capi.LDPC_F32_SP)
     ctx = capi.Context(capi.Code.from_tables(code), variant=variant, max_iter=10, max_row_metric=params["mrm"],
                        beta=params["beta"], llr_scale=params["scale"], max_abs_llr=params["max_abs"])
     key = fold_seeds(seeds)

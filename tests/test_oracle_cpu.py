@@ -32,6 +32,20 @@ def test_float_decoders_match_reference_golden(oracle, tag, mode, mrm, beta, cta
     assert np.array_equal(post.view(np.uint32), GOLD["%s_%s_post" % (tag, ctag)].view(np.uint32))
 
 
+@pytest.mark.parametrize("tag,mode,mrm,beta", [("f64sp", 1, 1e-16, 0.0), ("f64ms", 0, 31.0, 0.5)])
+@pytest.mark.parametrize("ctag,name", [("11ad", "11ad 1/2"), ("16e", "16e 1/2")])
+def test_double_decoders_match_reference_golden(oracle, tag, mode, mrm, beta, ctag, name):
+    """LDPCtop_Vec8d_prod / Vec8d_min: double posteriors bit for bit; the
+    reference's double LLRs are its float LLRs widened."""
+    from ldpc_b200 import codes
+    code = codes.make_code(name)
+    llr = GOLD["%s_%s_llr" % (tag, ctag)]
+    assert llr.dtype == np.float64 and np.array_equal(llr.astype(np.float32).astype(np.float64), llr)
+    post, it = oracle.decode_f64(code, llr, mode, 10, mrm, beta)
+    assert np.array_equal(it, GOLD["%s_%s_iters" % (tag, ctag)])
+    assert np.array_equal(post.view(np.uint64), GOLD["%s_%s_post" % (tag, ctag)].view(np.uint64))
+
+
 @pytest.mark.parametrize("tag,name", [("i8_11ad", "11ad 1/2"), ("i8_16e", "16e 1/2"), ("i8_11n81", "11n 1/2 z81")])
 def test_encoder_matches_reference_golden(oracle, tag, name):
     from ldpc_b200 import codes
