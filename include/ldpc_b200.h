@@ -193,9 +193,11 @@ int ldpc_decode_set_compat(ldpc_ctx *ctx, void *decoded_metrics, unsigned num_co
  * LDPC_F32_OMS).  int8 batches also take one int8 offset per layer (learned
  * offsets).  A plan fixes a list of jobs (device buffers
  * of one code each) and splits them into chunks of equal work.  A plan's
- * launch is ONE persistent kernel over all jobs, and it can be replayed
- * from a CUDA graph.  Per codeword, the results are exactly those of
- * ldpc_decode_int8 / ldpc_decode_count on that code. */
+ * launch is one persistent kernel over all jobs -- for int8 plans, one per
+ * geometry class: jobs whose codes would run at different occupancies get
+ * separate launches -- and it can be replayed from a CUDA graph (one kernel
+ * node per class, free to overlap).  Per codeword, the results are exactly
+ * those of ldpc_decode_int8 / ldpc_decode_count on that code. */
 typedef struct ldpc_batch ldpc_batch;
 typedef struct ldpc_batch_plan ldpc_batch_plan;
 
@@ -221,8 +223,9 @@ int ldpc_batch_create(const ldpc_code *const *codes, const ldpc_cfg *cfgs, int n
 int ldpc_batch_set_offsets(ldpc_batch *b, int code, const float *beta_per_layer);
 void ldpc_batch_destroy(ldpc_batch *b);
 
-/* Plan over `jobs`.  threads = CTA width (0: the autotuned or default value);
- * chunks_per_cta = work chunks per resident CTA (0: tuned or 2). */
+/* Plan over `jobs`.  threads = CTA width, for every class (0: the autotuned
+ * shapes, else max(256, the class's largest Z)); chunks_per_cta = work
+ * chunks per resident CTA (0: tuned or 2). */
 int ldpc_batch_plan_create(ldpc_batch *b, const ldpc_batch_job *jobs, int n_jobs, int threads, int chunks_per_cta,
                            ldpc_batch_plan **out);
 int ldpc_batch_plan_launch(ldpc_batch_plan *p, void *stream);
@@ -234,7 +237,10 @@ void ldpc_batch_plan_destroy(ldpc_batch_plan *p);
 /* Project autotuner: times plans over the first `sample` codewords of each
  * job (outputs not written) for every CTA width in {128..512} that fits and
  * 1, 2 or 4 chunks per CTA.  It keeps the fastest setting for later plans
- * and reports it (any output pointer may be NULL). */
+ * and reports it (any output pointer may be NULL).  int8 jobs of several
+ * geometry classes: each class is tuned on its own jobs, and that set is
+ * kept when it beats the best single shape on the whole sample; the report
+ * is then the shape of the slowest class and the whole sample's time. */
 int ldpc_batch_autotune(ldpc_batch *b, const ldpc_batch_job *jobs, int n_jobs, size_t sample, int *threads,
                         int *chunks_per_cta, double *ms);
 

@@ -1,6 +1,9 @@
 // Batched decoding: several codes (and Z sizes) in one persistent launch of
 // the run-time-table int8 kernel, plans with CUDA-graph replay, and the
-// launch-shape autotuner.
+// launch-shape autotuner.  An int8 plan whose codes would run at different
+// occupancies (shared memory, message placement, row-weight bucket) is split
+// into one persistent launch per class; its graph holds one kernel node per
+// class with no dependencies between them, so the classes overlap.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -20,7 +23,8 @@ struct ldpc_batch {
     std::vector<ldpc_cfg> cfgs;
     std::vector<std::vector<int>> beta8;     // per code, per layer
     std::vector<uint32_t> maxv2;
-    int tuned_threads = 0, tuned_cpc = 0;
+    int tuned_threads = 0, tuned_cpc = 0;    // one launch shape for all codes (float, or one class)
+    std::vector<int> code_threads, code_cpc;  // int8 per-class tuning, per code (0 = untuned)
 };
 
 struct ldpc_batch_plan {
@@ -39,6 +43,7 @@ struct ldpc_batch_plan {
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    std::vector<ldpc_batch_plan*> parts;      // per-class launches (owned); empty: this plan is one launch
 };
 
 namespace {
@@ -95,7 +100,19 @@ int check_job(const ldpc_batch* b, const ldpc_batch_job& j, int idx) {
     return LDPC_OK;
 }
 
+void release(ldpc_batch_plan* p);
+
+void destroy_plan(ldpc_batch_plan* p) {
+    if (p) {
+        cudaSetDevice(p->device);
+        release(p);
+        delete p;
+    }
+}
+
 void release(ldpc_batch_plan* p) {
+    for (ldpc_batch_plan* q : p->parts) destroy_plan(q);
+    p->parts.clear();
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
     if (p->ev_in) cudaEventDestroy(p->ev_in);
@@ -108,13 +125,7 @@ void release(ldpc_batch_plan* p) {
 }
 
 struct PlanDel {
-    void operator()(ldpc_batch_plan* p) const {
-        if (p) {
-            cudaSetDevice(p->device);
-            release(p);
-            delete p;
-        }
-    }
+    void operator()(ldpc_batch_plan* p) const { destroy_plan(p); }
 };
 
 int float_plan(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int threads, int cpc, ldpc_batch_plan** out) {
@@ -220,6 +231,211 @@ int float_plan(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int thread
     return LDPC_OK;
 }
 
+// One persistent launch of the run-time-table int8 kernel over the jobs; its
+// kernel variant, shared memory and message placement come from the codes
+// the jobs use.
+int int8_plan(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int threads, int cpc, ldpc_batch_plan** out) {
+    const int nc = (int)b->codes.size();
+    std::vector<char> used(nc, 0);
+    for (int i = 0; i < n_jobs; ++i) used[jobs[i].code] = 1;
+    std::vector<int> G(nc, 1);
+    int dmax = 8, maxE = 0;
+    bool quirk = false, rsmem = true;
+    for (int c = 0; c < nc; ++c) {
+        if (!used[c]) continue;
+        const ldpc_code& cd = b->codes[c];
+        const int n = cd.z * cd.mcol, E = (int)cd.row_cols.size();
+        G[c] = std::max(1, std::min(16, threads / cd.z));
+        while (G[c] > 1 && ldpc::rt_smem_bytes(n, G[c], E, 0, false) > (size_t)ldpc::kRtMaxSmem) --G[c];
+        if (ldpc::rt_smem_bytes(n, G[c], E, 0, false) > (size_t)ldpc::kRtMaxSmem)
+            return fail(LDPC_ERR_UNSUPPORTED, "batch plan: code %d (N=%d) does not fit shared memory", c, n);
+        if (ldpc::rt_smem_bytes(n, G[c], E, threads, true) > (size_t)ldpc::kRtMaxSmem) rsmem = false;
+        dmax = std::max(dmax, ldpc::rt_dmax(cd.max_row_weight));
+        maxE = std::max(maxE, E);
+        for (int v : b->beta8[c]) quirk |= v == 0;
+    }
+    size_t smem = 0;
+    for (int c = 0; c < nc; ++c) {
+        if (!used[c]) continue;
+        const ldpc_code& cd = b->codes[c];
+        smem = std::max(smem, ldpc::rt_smem_bytes(cd.z * cd.mcol, G[c], (int)cd.row_cols.size(), threads, rsmem));
+    }
+    std::unique_ptr<ldpc_batch_plan, PlanDel> p(new ldpc_batch_plan);
+    p->device = b->device;
+    p->k = ldpc::rt_kernel_for(dmax, quirk, rsmem);
+    p->threads = threads;
+    p->smem = (int)smem;
+    CUDA_TRY(ldpc::allow_dynamic_smem((const void*)p->k, ldpc::kRtMaxSmem));
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)p->k, threads, smem));
+    if (per_sm < 1) return fail(LDPC_ERR_UNSUPPORTED, "batch plan: %d threads x %zu B do not fit an SM", threads, smem);
+    const long long ctas = (long long)per_sm * b->sms;
+
+    std::vector<ldpc::RtCode> hc(nc);
+    for (int c = 0; c < nc; ++c) {
+        const ldpc_code& cd = b->codes[c];
+        if (int rc = ldpc::make_rt_code(cd, (int)b->cfgs[c].max_iter, b->maxv2[c], b->beta8[c].data(), 0, G[c], &hc[c]))
+            return rc;
+    }
+    std::vector<ldpc::RtJob> hj(n_jobs);
+    std::vector<long long> cost(n_jobs);
+    std::vector<int> minc(n_jobs);
+    for (int i = 0; i < n_jobs; ++i) {
+        const ldpc_batch_job& s = jobs[i];
+        ldpc::RtJob& j = hj[i];
+        memset(&j, 0, sizeof(j));
+        j.llr = (const int8_t*)s.llr;
+        j.ncw = (long long)s.n;
+        j.post_out = (int8_t*)s.post_out;
+        j.hard_out = s.hard_out;
+        j.iters_out = s.iters_out;
+        j.ref_bits = s.data_bits;
+        j.ref_period = s.ref_period > 0 ? (long long)s.ref_period : 1;
+        j.bucket_size = s.bucket_size > 0 ? (long long)s.bucket_size : std::max(1LL, (long long)s.n);
+        j.counters = s.counters;
+        j.n_buckets = std::max(1, std::min(s.n_buckets, ldpc::OMS_MAX_BUCKETS));
+        j.code = s.code;
+        const ldpc_code& cd = b->codes[s.code];
+        cost[i] = (long long)cd.row_cols.size() * cd.z;
+        minc[i] = 8 * G[s.code];     // a chunk keeps its 2G slots busy for a while
+    }
+    std::vector<ldpc::RtChunk> chunks;
+    std::vector<long long> ncw(n_jobs);
+    for (int i = 0; i < n_jobs; ++i) ncw[i] = hj[i].ncw;
+    make_chunks(ncw, cost, minc, ctas * cpc, chunks);
+    const int n_chunks = (int)chunks.size();
+    p->grid = (int)std::max(1LL, std::min<long long>(ctas, n_chunks));
+    CUDA_TRY(cudaMalloc(&p->d_codes, sizeof(ldpc::RtCode) * nc));
+    CUDA_TRY(cudaMemcpy(p->d_codes, hc.data(), sizeof(ldpc::RtCode) * nc, cudaMemcpyHostToDevice));
+    if (n_jobs) {
+        CUDA_TRY(cudaMalloc(&p->d_jobs, sizeof(ldpc::RtJob) * n_jobs));
+        CUDA_TRY(cudaMemcpy(p->d_jobs, hj.data(), sizeof(ldpc::RtJob) * n_jobs, cudaMemcpyHostToDevice));
+    }
+    if (n_chunks) {
+        CUDA_TRY(cudaMalloc(&p->d_chunks, sizeof(ldpc::RtChunk) * n_chunks));
+        CUDA_TRY(cudaMemcpy(p->d_chunks, chunks.data(), sizeof(ldpc::RtChunk) * n_chunks, cudaMemcpyHostToDevice));
+    }
+    long long words = 0;
+    if (!rsmem) {
+        words = (long long)maxE * threads;
+        CUDA_TRY(cudaMalloc(&p->d_scratch, (size_t)p->grid * words * 4));
+    }
+    memset(&p->lp, 0, sizeof(p->lp));
+    p->lp.codes = (const ldpc::RtCode*)p->d_codes;
+    p->lp.jobs = (const ldpc::RtJob*)p->d_jobs;
+    p->lp.chunks = p->d_chunks;
+    p->lp.n_chunks = n_chunks;
+    p->lp.r_scratch = (uint32_t*)p->d_scratch;
+    p->lp.r_words_per_cta = words;
+    if (!p->d_jobs) p->lp.n_chunks = 0;
+    p->n_chunks = p->lp.n_chunks;
+    *out = p.release();
+    return LDPC_OK;
+}
+
+// Occupancy class of a code decoded alone at `threads`: kernel variant,
+// message placement and CTAs per SM.
+struct Int8Class {
+    int dmax = 0, quirk = 0, rsmem = 0, per_sm = 0, threads = 0;
+    bool operator==(const Int8Class& o) const {
+        return dmax == o.dmax && quirk == o.quirk && rsmem == o.rsmem && per_sm == o.per_sm && threads == o.threads;
+    }
+};
+
+int int8_class(const ldpc_batch* b, int c, int threads, Int8Class* out) {
+    const ldpc_code& cd = b->codes[c];
+    const int n = cd.z * cd.mcol, E = (int)cd.row_cols.size();
+    int G = std::max(1, std::min(16, threads / cd.z));
+    while (G > 1 && ldpc::rt_smem_bytes(n, G, E, 0, false) > (size_t)ldpc::kRtMaxSmem) --G;
+    const bool rsmem = ldpc::rt_smem_bytes(n, G, E, threads, true) <= (size_t)ldpc::kRtMaxSmem;
+    bool quirk = false;
+    for (int v : b->beta8[c]) quirk |= v == 0;
+    const int dmax = ldpc::rt_dmax(cd.max_row_weight);
+    ldpc::rt_fn k = ldpc::rt_kernel_for(dmax, quirk, rsmem);
+    CUDA_TRY(ldpc::allow_dynamic_smem((const void*)k, ldpc::kRtMaxSmem));
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k, threads,
+                                                           ldpc::rt_smem_bytes(n, G, E, threads, rsmem)));
+    out->dmax = dmax;
+    out->quirk = quirk;
+    out->rsmem = rsmem;
+    out->per_sm = per_sm;
+    out->threads = threads;
+    return LDPC_OK;
+}
+
+// Class index of every code used by the jobs (code_cls[c], -1 if unused);
+// returns the number of classes.  Widths: `threads` when explicit, else each
+// code's default max(256, Z rounded to 32).
+int int8_classes(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, bool explicit_threads, int threads,
+                 std::vector<int>& code_cls, int* n_cls) {
+    const int nc = (int)b->codes.size();
+    std::vector<Int8Class> cls;
+    code_cls.assign(nc, -1);
+    for (int i = 0; i < n_jobs; ++i) {
+        const int c = jobs[i].code;
+        if (code_cls[c] >= 0) continue;
+        Int8Class k;
+        const int t = explicit_threads ? threads : std::max(256, ((b->codes[c].z + 31) / 32) * 32);
+        if (int rc = int8_class(b, c, t, &k)) return rc;
+        int idx = -1;
+        for (size_t j = 0; j < cls.size(); ++j)
+            if (cls[j] == k) idx = (int)j;
+        if (idx < 0) {
+            idx = (int)cls.size();
+            cls.push_back(k);
+        }
+        code_cls[c] = idx;
+    }
+    *n_cls = (int)cls.size();
+    return LDPC_OK;
+}
+
+// The jobs of class k, and their largest Z.
+std::vector<ldpc_batch_job> class_jobs(const ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs,
+                                       const std::vector<int>& code_cls, int k, int* maxz) {
+    std::vector<ldpc_batch_job> sub;
+    *maxz = 0;
+    for (int i = 0; i < n_jobs; ++i)
+        if (code_cls[jobs[i].code] == k) {
+            sub.push_back(jobs[i]);
+            *maxz = std::max(*maxz, b->codes[jobs[i].code].z);
+        }
+    return sub;
+}
+
+// The jobs grouped by the occupancy class of their code; one launch per
+// class (a single launch when there is one class, or when LDPC_BATCH_ONE_LAUNCH
+// is set).  threads: the caller's width, applied to every class when
+// explicit; otherwise each class takes its tuned shape (ldpc_batch_autotune)
+// or max(256, its largest Z rounded to 32) and `cpc`.
+int int8_plan_classes(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, bool explicit_threads, int threads,
+                      int cpc, ldpc_batch_plan** out) {
+    if (getenv("LDPC_BATCH_ONE_LAUNCH") || n_jobs < 2) return int8_plan(b, jobs, n_jobs, threads, cpc, out);
+    std::vector<int> code_cls;
+    int n_cls = 0;
+    if (int rc = int8_classes(b, jobs, n_jobs, explicit_threads, threads, code_cls, &n_cls)) return rc;
+    if (n_cls < 2) return int8_plan(b, jobs, n_jobs, threads, cpc, out);
+    std::unique_ptr<ldpc_batch_plan, PlanDel> p(new ldpc_batch_plan);
+    p->device = b->device;
+    for (int k = 0; k < n_cls; ++k) {
+        int maxz = 0;
+        std::vector<ldpc_batch_job> sub = class_jobs(b, jobs, n_jobs, code_cls, k, &maxz);
+        int t = explicit_threads ? threads : std::max(256, ((maxz + 31) / 32) * 32);
+        int c = cpc;
+        if (!explicit_threads && !b->code_threads.empty() && b->code_threads[sub[0].code] >= maxz) {
+            t = b->code_threads[sub[0].code];
+            c = b->code_cpc[sub[0].code];
+        }
+        ldpc_batch_plan* part = nullptr;
+        if (int rc = int8_plan(b, sub.data(), (int)sub.size(), t, c, &part)) return rc;
+        p->parts.push_back(part);
+        p->n_chunks += part->n_chunks;
+    }
+    *out = p.release();
+    return LDPC_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -297,115 +513,29 @@ int ldpc_batch_plan_create(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs
     for (int i = 0; i < n_jobs; ++i)
         if (int rc = check_job(b, jobs[i], i)) return rc;
     CUDA_TRY(cudaSetDevice(b->device));
-    // codes used by the jobs
-    const int nc = (int)b->codes.size();
     int maxz = 0;
     for (int i = 0; i < n_jobs; ++i) maxz = std::max(maxz, b->codes[jobs[i].code].z);
     if (threads <= 0) threads = b->tuned_threads;
+    const bool explicit_threads = threads > 0;
     if (threads <= 0) threads = std::max(256, ((maxz + 31) / 32) * 32);
     if (cpc <= 0) cpc = b->tuned_cpc > 0 ? b->tuned_cpc : 2;
     if (threads % 32 || threads > ldpc::kRtMaxThreads || threads < maxz)
         return fail(LDPC_ERR_UNSUPPORTED, "batch plan: %d threads per CTA (multiple of 32, >= Z=%d, <= %d)", threads, maxz,
                     ldpc::kRtMaxThreads);
     if (b->variant != LDPC_INT8_OMS) return float_plan(b, jobs, n_jobs, threads, cpc, out);
-    std::vector<int> G(nc, 1);
-    int dmax = 8, maxE = 0;
-    bool quirk = false, rsmem = true;
-    for (int c = 0; c < nc; ++c) {
-        const ldpc_code& cd = b->codes[c];
-        const int n = cd.z * cd.mcol, E = (int)cd.row_cols.size();
-        G[c] = std::max(1, std::min(16, threads / cd.z));
-        while (G[c] > 1 && ldpc::rt_smem_bytes(n, G[c], E, 0, false) > (size_t)ldpc::kRtMaxSmem) --G[c];
-        if (ldpc::rt_smem_bytes(n, G[c], E, 0, false) > (size_t)ldpc::kRtMaxSmem)
-            return fail(LDPC_ERR_UNSUPPORTED, "batch plan: code %d (N=%d) does not fit shared memory", c, n);
-        if (ldpc::rt_smem_bytes(n, G[c], E, threads, true) > (size_t)ldpc::kRtMaxSmem) rsmem = false;
-        dmax = std::max(dmax, ldpc::rt_dmax(cd.max_row_weight));
-        maxE = std::max(maxE, E);
-        for (int v : b->beta8[c]) quirk |= v == 0;
-    }
-    size_t smem = 0;
-    for (int c = 0; c < nc; ++c) {
-        const ldpc_code& cd = b->codes[c];
-        smem = std::max(smem, ldpc::rt_smem_bytes(cd.z * cd.mcol, G[c], (int)cd.row_cols.size(), threads, rsmem));
-    }
-    std::unique_ptr<ldpc_batch_plan, PlanDel> p(new ldpc_batch_plan);
-    p->device = b->device;
-    p->k = ldpc::rt_kernel_for(dmax, quirk, rsmem);
-    p->threads = threads;
-    p->smem = (int)smem;
-    CUDA_TRY(ldpc::allow_dynamic_smem((const void*)p->k, ldpc::kRtMaxSmem));
-    int per_sm = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)p->k, threads, smem));
-    if (per_sm < 1) return fail(LDPC_ERR_UNSUPPORTED, "batch plan: %d threads x %zu B do not fit an SM", threads, smem);
-    const long long ctas = (long long)per_sm * b->sms;
-
-    std::vector<ldpc::RtCode> hc(nc);
-    for (int c = 0; c < nc; ++c) {
-        const ldpc_code& cd = b->codes[c];
-        if (int rc = ldpc::make_rt_code(cd, (int)b->cfgs[c].max_iter, b->maxv2[c], b->beta8[c].data(), 0, G[c], &hc[c]))
-            return rc;
-    }
-    std::vector<ldpc::RtJob> hj(n_jobs);
-    std::vector<long long> cost(n_jobs);
-    std::vector<int> minc(n_jobs);
-    for (int i = 0; i < n_jobs; ++i) {
-        const ldpc_batch_job& s = jobs[i];
-        ldpc::RtJob& j = hj[i];
-        memset(&j, 0, sizeof(j));
-        j.llr = (const int8_t*)s.llr;
-        j.ncw = (long long)s.n;
-        j.post_out = (int8_t*)s.post_out;
-        j.hard_out = s.hard_out;
-        j.iters_out = s.iters_out;
-        j.ref_bits = s.data_bits;
-        j.ref_period = s.ref_period > 0 ? (long long)s.ref_period : 1;
-        j.bucket_size = s.bucket_size > 0 ? (long long)s.bucket_size : std::max(1LL, (long long)s.n);
-        j.counters = s.counters;
-        j.n_buckets = std::max(1, std::min(s.n_buckets, ldpc::OMS_MAX_BUCKETS));
-        j.code = s.code;
-        const ldpc_code& cd = b->codes[s.code];
-        cost[i] = (long long)cd.row_cols.size() * cd.z;
-        minc[i] = 8 * G[s.code];     // a chunk keeps its 2G slots busy for a while
-    }
-    std::vector<ldpc::RtChunk> chunks;
-    std::vector<long long> ncw(n_jobs);
-    for (int i = 0; i < n_jobs; ++i) ncw[i] = hj[i].ncw;
-    make_chunks(ncw, cost, minc, ctas * cpc, chunks);
-    const int n_chunks = (int)chunks.size();
-    p->grid = (int)std::max(1LL, std::min<long long>(ctas, n_chunks));
-    CUDA_TRY(cudaMalloc(&p->d_codes, sizeof(ldpc::RtCode) * nc));
-    CUDA_TRY(cudaMemcpy(p->d_codes, hc.data(), sizeof(ldpc::RtCode) * nc, cudaMemcpyHostToDevice));
-    if (n_jobs) {
-        CUDA_TRY(cudaMalloc(&p->d_jobs, sizeof(ldpc::RtJob) * n_jobs));
-        CUDA_TRY(cudaMemcpy(p->d_jobs, hj.data(), sizeof(ldpc::RtJob) * n_jobs, cudaMemcpyHostToDevice));
-    }
-    if (n_chunks) {
-        CUDA_TRY(cudaMalloc(&p->d_chunks, sizeof(ldpc::RtChunk) * n_chunks));
-        CUDA_TRY(cudaMemcpy(p->d_chunks, chunks.data(), sizeof(ldpc::RtChunk) * n_chunks, cudaMemcpyHostToDevice));
-    }
-    long long words = 0;
-    if (!rsmem) {
-        words = (long long)maxE * threads;
-        CUDA_TRY(cudaMalloc(&p->d_scratch, (size_t)p->grid * words * 4));
-    }
-    memset(&p->lp, 0, sizeof(p->lp));
-    p->lp.codes = (const ldpc::RtCode*)p->d_codes;
-    p->lp.jobs = (const ldpc::RtJob*)p->d_jobs;
-    p->lp.chunks = p->d_chunks;
-    p->lp.n_chunks = n_chunks;
-    p->lp.r_scratch = (uint32_t*)p->d_scratch;
-    p->lp.r_words_per_cta = words;
-    if (!p->d_jobs) p->lp.n_chunks = 0;
-    p->n_chunks = p->lp.n_chunks;
-    *out = p.release();
-    return LDPC_OK;
+    return int8_plan_classes(b, jobs, n_jobs, explicit_threads, threads, cpc, out);
 }
 
 int ldpc_batch_plan_launch(ldpc_batch_plan* p, void* stream) {
     if (!p) return fail(LDPC_ERR_INVALID_ARG, "plan is NULL");
     if (p->n_chunks == 0) return LDPC_OK;
     CUDA_TRY(cudaSetDevice(p->device));
-    launch_plan_kernel(p, (cudaStream_t)stream);
+    if (p->parts.empty()) {
+        launch_plan_kernel(p, (cudaStream_t)stream);
+    } else {
+        for (ldpc_batch_plan* q : p->parts)
+            if (q->n_chunks) launch_plan_kernel(q, (cudaStream_t)stream);
+    }
     CUDA_TRY(cudaGetLastError());
     return LDPC_OK;
 }
@@ -415,20 +545,36 @@ int ldpc_batch_plan_graph_launch(ldpc_batch_plan* p, void* stream) {
     if (p->n_chunks == 0) return LDPC_OK;
     CUDA_TRY(cudaSetDevice(p->device));
     if (!p->exec) {
-        CUDA_TRY(cudaStreamCreateWithFlags(&p->own, cudaStreamNonBlocking));
-        CUDA_TRY(cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming));
-        CUDA_TRY(cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming));
-        CUDA_TRY(cudaStreamBeginCapture(p->own, cudaStreamCaptureModeThreadLocal));
-        launch_plan_kernel(p, p->own);
-        const cudaError_t le = cudaGetLastError();
+        if (!p->own) CUDA_TRY(cudaStreamCreateWithFlags(&p->own, cudaStreamNonBlocking));
+        if (!p->ev_in) CUDA_TRY(cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming));
+        if (!p->ev_out) CUDA_TRY(cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming));
+        // one kernel node per launch of the plan, with no edges between them:
+        // the per-class launches may run side by side
         cudaGraph_t g = nullptr;
-        const cudaError_t ce = cudaStreamEndCapture(p->own, &g);
-        if (le != cudaSuccess || ce != cudaSuccess) {
-            if (g) cudaGraphDestroy(g);
-            return fail(LDPC_ERR_CUDA, "graph capture: %s", cudaGetErrorString(le != cudaSuccess ? le : ce));
+        CUDA_TRY(cudaGraphCreate(&g, 0));
+        std::vector<ldpc_batch_plan*> leaves = p->parts;
+        if (leaves.empty()) leaves.push_back(p);
+        cudaError_t e = cudaSuccess;
+        for (ldpc_batch_plan* q : leaves) {
+            if (!q->n_chunks) continue;
+            void* arg = q->is_float ? (void*)&q->slp : (void*)&q->lp;
+            cudaKernelNodeParams kp;
+            memset(&kp, 0, sizeof(kp));
+            kp.func = q->is_float ? q->kf : (void*)q->k;
+            kp.gridDim = dim3((unsigned)q->grid);
+            kp.blockDim = dim3((unsigned)q->threads);
+            kp.sharedMemBytes = (unsigned)q->smem;
+            kp.kernelParams = &arg;
+            cudaGraphNode_t node;
+            if ((e = cudaGraphAddKernelNode(&node, g, nullptr, 0, &kp)) != cudaSuccess) break;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, g, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(g);
+            p->exec = nullptr;
+            return fail(LDPC_ERR_CUDA, "plan graph: %s", cudaGetErrorString(e));
         }
         p->graph = g;
-        CUDA_TRY(cudaGraphInstantiate(&p->exec, p->graph, 0));
     }
     // replay on the plan's stream, ordered after and before the caller's stream
     CUDA_TRY(cudaEventRecord(p->ev_in, (cudaStream_t)stream));
@@ -440,6 +586,62 @@ int ldpc_batch_plan_graph_launch(ldpc_batch_plan* p, void* stream) {
 }
 
 void ldpc_batch_plan_destroy(ldpc_batch_plan* p) { PlanDel()(p); }
+
+}  // extern "C"
+
+namespace {
+// Median of three timed launches (after a warm-up) of a plan over the jobs
+// at width t and c chunks per CTA (t = 0: the batch's per-class shapes);
+// *ms_out < 0 when the shape does not fit.
+int time_shape(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int t, int c, cudaStream_t s, cudaEvent_t e0,
+               cudaEvent_t e1, double* ms_out) {
+    *ms_out = -1;
+    ldpc_batch_plan* p = nullptr;
+    if (ldpc_batch_plan_create(b, jobs, n_jobs, t, c, &p) != LDPC_OK) return LDPC_OK;   // shape does not fit
+    float ms[3] = {0, 0, 0};
+    int rc = ldpc_batch_plan_launch(p, s);    // warm-up
+    for (int r = 0; r < 3 && rc == LDPC_OK; ++r) {
+        cudaEventRecord(e0, s);
+        rc = ldpc_batch_plan_launch(p, s);
+        cudaEventRecord(e1, s);
+        if (cudaEventSynchronize(e1) != cudaSuccess) rc = fail(LDPC_ERR_CUDA, "autotune: launch failed");
+        else cudaEventElapsedTime(&ms[r], e0, e1);
+    }
+    ldpc_batch_plan_destroy(p);
+    if (rc != LDPC_OK) return rc;
+    std::sort(ms, ms + 3);
+    *ms_out = ms[1];
+    return LDPC_OK;
+}
+
+// The fastest (width, chunks per CTA) for these jobs: every width of
+// kTunedWidths >= maxz and 1, 2 or 4 chunks per CTA.
+int tune_shape(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int maxz, cudaStream_t s, cudaEvent_t e0,
+               cudaEvent_t e1, int* t_out, int* c_out, double* ms_out) {
+    double best = 1e30;
+    int best_t = 0, best_c = 0;
+    const int cpcs[] = {1, 2, 4};
+    for (int t : kTunedWidths) {
+        if (t < maxz) continue;
+        for (int c : cpcs) {
+            double ms = 0;
+            if (int rc = time_shape(b, jobs, n_jobs, t, c, s, e0, e1, &ms)) return rc;
+            if (ms >= 0 && ms < best) {
+                best = ms;
+                best_t = t;
+                best_c = c;
+            }
+        }
+    }
+    if (!best_t) return fail(LDPC_ERR_UNSUPPORTED, "autotune: no launch shape fits these codes");
+    *t_out = best_t;
+    *c_out = best_c;
+    *ms_out = best;
+    return LDPC_OK;
+}
+}  // namespace
+
+extern "C" {
 
 int ldpc_batch_autotune(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, size_t sample, int* threads_out,
                         int* cpc_out, double* ms_out) {
@@ -464,41 +666,70 @@ int ldpc_batch_autotune(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, s
     CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));
-    double best = 1e30;
-    int best_t = 0, best_c = 0, rc = LDPC_OK;
-    const int cpcs[] = {1, 2, 4};
-    for (int t : kTunedWidths) {
-        if (t < maxz) continue;
-        for (int c : cpcs) {
-            ldpc_batch_plan* p = nullptr;
-            if (ldpc_batch_plan_create(b, sj.data(), n_jobs, t, c, &p) != LDPC_OK) continue;   // shape does not fit
-            float ms[3] = {0, 0, 0};
-            rc = ldpc_batch_plan_launch(p, s);    // warm-up
-            for (int r = 0; r < 3 && rc == LDPC_OK; ++r) {
-                cudaEventRecord(e0, s);
-                rc = ldpc_batch_plan_launch(p, s);
-                cudaEventRecord(e1, s);
-                if (cudaEventSynchronize(e1) != cudaSuccess) rc = fail(LDPC_ERR_CUDA, "autotune: launch failed");
-                else cudaEventElapsedTime(&ms[r], e0, e1);
-            }
-            ldpc_batch_plan_destroy(p);
+    int rc = LDPC_OK;
+    std::vector<int> code_cls;
+    int n_cls = 1;
+    if (b->variant == LDPC_INT8_OMS && !getenv("LDPC_BATCH_ONE_LAUNCH") && n_jobs > 1)
+        rc = int8_classes(b, sj.data(), n_jobs, false, 0, code_cls, &n_cls);
+    double best = 1e30, worst = -1;
+    int best_t = 0, best_c = 0;
+    if (rc == LDPC_OK && n_cls > 1) {
+        // int8 classes: each class is its own launch.  Candidates: every class
+        // tuned on its own jobs, and one shape for all classes; the whole
+        // sample plan decides between them.
+        std::vector<int> ct(b->codes.size(), 0), cc(b->codes.size(), 0);
+        for (int k = 0; k < n_cls && rc == LDPC_OK; ++k) {
+            int kz = 0, t = 0, c = 0;
+            double ms = 0;
+            std::vector<ldpc_batch_job> sub = class_jobs(b, sj.data(), n_jobs, code_cls, k, &kz);
+            rc = tune_shape(b, sub.data(), (int)sub.size(), kz, s, e0, e1, &t, &c, &ms);
             if (rc != LDPC_OK) break;
-            std::sort(ms, ms + 3);
-            if (ms[1] < best) {
-                best = ms[1];
+            for (const ldpc_batch_job& j : sub) {
+                ct[j.code] = t;
+                cc[j.code] = c;
+            }
+            if (ms > worst) {
+                worst = ms;
                 best_t = t;
                 best_c = c;
             }
         }
-        if (rc != LDPC_OK) break;
+        double ms_pc = -1, ms_glob = 0;
+        int gt = 0, gc = 0;
+        if (rc == LDPC_OK) {
+            b->code_threads = ct;
+            b->code_cpc = cc;
+            b->tuned_threads = b->tuned_cpc = 0;
+            rc = time_shape(b, sj.data(), n_jobs, 0, 0, s, e0, e1, &ms_pc);
+        }
+        if (rc == LDPC_OK) rc = tune_shape(b, sj.data(), n_jobs, maxz, s, e0, e1, &gt, &gc, &ms_glob);
+        if (rc == LDPC_OK) {
+            if (ms_pc < 0 || ms_glob < ms_pc) {
+                b->tuned_threads = best_t = gt;
+                b->tuned_cpc = best_c = gc;
+                b->code_threads.clear();
+                b->code_cpc.clear();
+                best = ms_glob;
+            } else {
+                best = ms_pc;
+            }
+        } else {
+            b->code_threads.clear();
+            b->code_cpc.clear();
+        }
+    } else if (rc == LDPC_OK) {
+        rc = tune_shape(b, sj.data(), n_jobs, maxz, s, e0, e1, &best_t, &best_c, &best);
+        if (rc == LDPC_OK) {
+            b->tuned_threads = best_t;
+            b->tuned_cpc = best_c;
+            b->code_threads.clear();
+            b->code_cpc.clear();
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaStreamDestroy(s);
     if (rc != LDPC_OK) return rc;
-    if (!best_t) return fail(LDPC_ERR_UNSUPPORTED, "autotune: no launch shape fits these codes");
-    b->tuned_threads = best_t;
-    b->tuned_cpc = best_c;
     if (threads_out) *threads_out = best_t;
     if (cpc_out) *cpc_out = best_c;
     if (ms_out) *ms_out = best;
