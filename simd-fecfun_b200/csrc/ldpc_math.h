@@ -7,10 +7,12 @@
  * reference tree.  Near the clamp (1 - 2^-24) one ulp of the product moves
  * 2*atanh by ~0.7, so the GPU decoder and the CPU oracle must use the *same*
  * function, bit for bit.  This header is that function.  It uses only IEEE
- * single-precision +, -, *, / and round-to-nearest-even, written so that no
- * compiler may contract them into fused multiply-adds:
- *   - device code calls __fmul_rn/__fadd_rn/__fsub_rn/__fdiv_rn;
- *   - host code must be compiled with -ffp-contract=off.
+ * single-precision +, -, *, /, fused multiply-add and round-to-nearest-even,
+ * each correctly rounded, written so that no compiler may contract or
+ * reassociate them:
+ *   - device code calls __fmul_rn/__fadd_rn/__fsub_rn/__fdiv_rn/__fmaf_rn;
+ *   - host code calls fmaf for the fused steps and must be compiled with
+ *     -ffp-contract=off for the others.
  *
  * Methods (from the mathematics, not from any library):
  *   expm1(y), y <= 0:  |y| < 1/4: Taylor series to y^9;
@@ -40,11 +42,14 @@
 #define LM_ADD(a, b) __fadd_rn((a), (b))
 #define LM_SUB(a, b) __fsub_rn((a), (b))
 #define LM_DIV(a, b) __fdiv_rn((a), (b))
+#define LM_FMA(a, b, c) __fmaf_rn((a), (b), (c))
 #else
+#include <math.h>
 #define LM_MUL(a, b) ((float)(a) * (float)(b))
 #define LM_ADD(a, b) ((float)(a) + (float)(b))
 #define LM_SUB(a, b) ((float)(a) - (float)(b))
 #define LM_DIV(a, b) ((float)(a) / (float)(b))
+#define LM_FMA(a, b, c) fmaf((float)(a), (float)(b), (float)(c))
 #endif
 
 LM_FN int32_t lm_f2i(float x) {
@@ -75,17 +80,17 @@ LM_FN float lm_exp_neg(float y) {
     const float ln2_hi = 0.693145751953125f;          /* 12 significant bits: k*ln2_hi exact */
     const float ln2_lo = 1.428606765330187045e-06f;
     float k = lm_rint(LM_MUL(y, inv_ln2));
-    float r = LM_SUB(LM_SUB(y, LM_MUL(k, ln2_hi)), LM_MUL(k, ln2_lo));
+    float r = LM_FMA(-k, ln2_lo, LM_FMA(-k, ln2_hi, y));
     /* e^r, |r| <= 0.35, Taylor to r^8 (Horner) */
     float p = 2.4801587301587302e-05f;                 /* 1/8! */
-    p = LM_ADD(LM_MUL(p, r), 1.9841269841269841e-04f); /* 1/7! */
-    p = LM_ADD(LM_MUL(p, r), 1.3888888888888889e-03f); /* 1/6! */
-    p = LM_ADD(LM_MUL(p, r), 8.3333333333333333e-03f); /* 1/5! */
-    p = LM_ADD(LM_MUL(p, r), 4.1666666666666667e-02f); /* 1/4! */
-    p = LM_ADD(LM_MUL(p, r), 1.6666666666666667e-01f); /* 1/3! */
-    p = LM_ADD(LM_MUL(p, r), 0.5f);
-    p = LM_ADD(LM_MUL(p, r), 1.0f);
-    p = LM_ADD(LM_MUL(p, r), 1.0f);
+    p = LM_FMA(p, r, 1.9841269841269841e-04f); /* 1/7! */
+    p = LM_FMA(p, r, 1.3888888888888889e-03f); /* 1/6! */
+    p = LM_FMA(p, r, 8.3333333333333333e-03f); /* 1/5! */
+    p = LM_FMA(p, r, 4.1666666666666667e-02f); /* 1/4! */
+    p = LM_FMA(p, r, 1.6666666666666667e-01f); /* 1/3! */
+    p = LM_FMA(p, r, 0.5f);
+    p = LM_FMA(p, r, 1.0f);
+    p = LM_FMA(p, r, 1.0f);
     int32_t ki = (int32_t)k;                          /* -44 <= ki <= 0 */
     return LM_MUL(p, lm_i2f((127 + ki) << 23));
 }
@@ -94,14 +99,14 @@ LM_FN float lm_exp_neg(float y) {
 LM_FN float lm_expm1_neg(float y) {
     if (y > -0.25f) {
         float p = 2.7557319223985891e-06f;                 /* 1/9! */
-        p = LM_ADD(LM_MUL(p, y), 2.4801587301587302e-05f); /* 1/8! */
-        p = LM_ADD(LM_MUL(p, y), 1.9841269841269841e-04f);
-        p = LM_ADD(LM_MUL(p, y), 1.3888888888888889e-03f);
-        p = LM_ADD(LM_MUL(p, y), 8.3333333333333333e-03f);
-        p = LM_ADD(LM_MUL(p, y), 4.1666666666666667e-02f);
-        p = LM_ADD(LM_MUL(p, y), 1.6666666666666667e-01f);
-        p = LM_ADD(LM_MUL(p, y), 0.5f);
-        p = LM_ADD(LM_MUL(p, y), 1.0f);
+        p = LM_FMA(p, y, 2.4801587301587302e-05f); /* 1/8! */
+        p = LM_FMA(p, y, 1.9841269841269841e-04f);
+        p = LM_FMA(p, y, 1.3888888888888889e-03f);
+        p = LM_FMA(p, y, 8.3333333333333333e-03f);
+        p = LM_FMA(p, y, 4.1666666666666667e-02f);
+        p = LM_FMA(p, y, 1.6666666666666667e-01f);
+        p = LM_FMA(p, y, 0.5f);
+        p = LM_FMA(p, y, 1.0f);
         return LM_MUL(p, y);
     }
     return LM_SUB(lm_exp_neg(y), 1.0f);
@@ -118,12 +123,12 @@ LM_FN float lm_tanh_pos(float x) {
 LM_FN float lm_log_series(float s) {
     float s2 = LM_MUL(s, s);
     float p = 7.6923076923076923e-02f;            /* 1/13 */
-    p = LM_ADD(LM_MUL(p, s2), 9.0909090909090909e-02f);
-    p = LM_ADD(LM_MUL(p, s2), 1.1111111111111111e-01f);
-    p = LM_ADD(LM_MUL(p, s2), 1.4285714285714286e-01f);
-    p = LM_ADD(LM_MUL(p, s2), 2.0000000000000000e-01f);
-    p = LM_ADD(LM_MUL(p, s2), 3.3333333333333333e-01f);
-    p = LM_ADD(LM_MUL(p, s2), 1.0f);
+    p = LM_FMA(p, s2, 9.0909090909090909e-02f);
+    p = LM_FMA(p, s2, 1.1111111111111111e-01f);
+    p = LM_FMA(p, s2, 1.4285714285714286e-01f);
+    p = LM_FMA(p, s2, 2.0000000000000000e-01f);
+    p = LM_FMA(p, s2, 3.3333333333333333e-01f);
+    p = LM_FMA(p, s2, 1.0f);
     return LM_MUL(2.0f, LM_MUL(p, s));
 }
 
@@ -142,8 +147,8 @@ LM_FN float lm_log1p_pos(float t) {
     float s = LM_DIV(LM_SUB(f, 1.0f), LM_ADD(f, 1.0f));
     float ef = (float)e;
     float corr = LM_DIV(LM_SUB(t, LM_SUB(u, 1.0f)), u);
-    float lo = LM_ADD(LM_ADD(LM_MUL(ef, ln2_lo), lm_log_series(s)), corr);
-    return LM_ADD(LM_MUL(ef, ln2_hi), lo);
+    float lo = LM_ADD(LM_FMA(ef, ln2_lo, lm_log_series(s)), corr);
+    return LM_FMA(ef, ln2_hi, lo);
 }
 
 /* atanh(m) for 0 <= m < 1 */
@@ -178,11 +183,13 @@ LM_FN float lm_atanh(float m) {
 #define LMD_ADD(a, b) __dadd_rn((a), (b))
 #define LMD_SUB(a, b) __dsub_rn((a), (b))
 #define LMD_DIV(a, b) __ddiv_rn((a), (b))
+#define LMD_FMA(a, b, c) __fma_rn((a), (b), (c))
 #else
 #define LMD_MUL(a, b) ((double)(a) * (double)(b))
 #define LMD_ADD(a, b) ((double)(a) + (double)(b))
 #define LMD_SUB(a, b) ((double)(a) - (double)(b))
 #define LMD_DIV(a, b) ((double)(a) / (double)(b))
+#define LMD_FMA(a, b, c) fma((double)(a), (double)(b), (double)(c))
 #endif
 
 LM_FN int64_t lmd_d2i(double x) {
@@ -214,22 +221,22 @@ LM_FN double lmd_rint(double x) {
 LM_FN double lmd_exp_neg(double y) {
     const double inv_ln2 = 1.4426950408889634;
     double k = lmd_rint(LMD_MUL(y, inv_ln2));
-    double r = LMD_SUB(LMD_SUB(y, LMD_MUL(k, LMD_LN2_HI)), LMD_MUL(k, LMD_LN2_LO));
+    double r = LMD_FMA(-k, LMD_LN2_LO, LMD_FMA(-k, LMD_LN2_HI, y));
     double p = 1.1470745597729725e-11;                   /* 1/14! */
-    p = LMD_ADD(LMD_MUL(p, r), 1.6059043836821613e-10); /* 1/13! */
-    p = LMD_ADD(LMD_MUL(p, r), 2.08767569878681e-09);   /* 1/12! */
-    p = LMD_ADD(LMD_MUL(p, r), 2.505210838544172e-08);  /* 1/11! */
-    p = LMD_ADD(LMD_MUL(p, r), 2.7557319223985888e-07); /* 1/10! */
-    p = LMD_ADD(LMD_MUL(p, r), 2.7557319223985893e-06); /* 1/9! */
-    p = LMD_ADD(LMD_MUL(p, r), 2.4801587301587302e-05); /* 1/8! */
-    p = LMD_ADD(LMD_MUL(p, r), 1.9841269841269841e-04); /* 1/7! */
-    p = LMD_ADD(LMD_MUL(p, r), 1.3888888888888889e-03); /* 1/6! */
-    p = LMD_ADD(LMD_MUL(p, r), 8.3333333333333332e-03); /* 1/5! */
-    p = LMD_ADD(LMD_MUL(p, r), 4.1666666666666664e-02); /* 1/4! */
-    p = LMD_ADD(LMD_MUL(p, r), 1.6666666666666666e-01); /* 1/3! */
-    p = LMD_ADD(LMD_MUL(p, r), 0.5);
-    p = LMD_ADD(LMD_MUL(p, r), 1.0);
-    p = LMD_ADD(LMD_MUL(p, r), 1.0);
+    p = LMD_FMA(p, r, 1.6059043836821613e-10); /* 1/13! */
+    p = LMD_FMA(p, r, 2.08767569878681e-09);   /* 1/12! */
+    p = LMD_FMA(p, r, 2.505210838544172e-08);  /* 1/11! */
+    p = LMD_FMA(p, r, 2.7557319223985888e-07); /* 1/10! */
+    p = LMD_FMA(p, r, 2.7557319223985893e-06); /* 1/9! */
+    p = LMD_FMA(p, r, 2.4801587301587302e-05); /* 1/8! */
+    p = LMD_FMA(p, r, 1.9841269841269841e-04); /* 1/7! */
+    p = LMD_FMA(p, r, 1.3888888888888889e-03); /* 1/6! */
+    p = LMD_FMA(p, r, 8.3333333333333332e-03); /* 1/5! */
+    p = LMD_FMA(p, r, 4.1666666666666664e-02); /* 1/4! */
+    p = LMD_FMA(p, r, 1.6666666666666666e-01); /* 1/3! */
+    p = LMD_FMA(p, r, 0.5);
+    p = LMD_FMA(p, r, 1.0);
+    p = LMD_FMA(p, r, 1.0);
     int64_t ki = (int64_t)k;                             /* -65 <= ki <= 0 */
     return LMD_MUL(p, lmd_i2d((int64_t)(1023 + ki) << 52));
 }
@@ -238,19 +245,19 @@ LM_FN double lmd_exp_neg(double y) {
 LM_FN double lmd_expm1_neg(double y) {
     if (y > -0.25) {
         double p = 1.1470745597729725e-11;                   /* 1/14! */
-        p = LMD_ADD(LMD_MUL(p, y), 1.6059043836821613e-10);
-        p = LMD_ADD(LMD_MUL(p, y), 2.08767569878681e-09);
-        p = LMD_ADD(LMD_MUL(p, y), 2.505210838544172e-08);
-        p = LMD_ADD(LMD_MUL(p, y), 2.7557319223985888e-07);
-        p = LMD_ADD(LMD_MUL(p, y), 2.7557319223985893e-06);
-        p = LMD_ADD(LMD_MUL(p, y), 2.4801587301587302e-05);
-        p = LMD_ADD(LMD_MUL(p, y), 1.9841269841269841e-04);
-        p = LMD_ADD(LMD_MUL(p, y), 1.3888888888888889e-03);
-        p = LMD_ADD(LMD_MUL(p, y), 8.3333333333333332e-03);
-        p = LMD_ADD(LMD_MUL(p, y), 4.1666666666666664e-02);
-        p = LMD_ADD(LMD_MUL(p, y), 1.6666666666666666e-01);
-        p = LMD_ADD(LMD_MUL(p, y), 0.5);
-        p = LMD_ADD(LMD_MUL(p, y), 1.0);
+        p = LMD_FMA(p, y, 1.6059043836821613e-10);
+        p = LMD_FMA(p, y, 2.08767569878681e-09);
+        p = LMD_FMA(p, y, 2.505210838544172e-08);
+        p = LMD_FMA(p, y, 2.7557319223985888e-07);
+        p = LMD_FMA(p, y, 2.7557319223985893e-06);
+        p = LMD_FMA(p, y, 2.4801587301587302e-05);
+        p = LMD_FMA(p, y, 1.9841269841269841e-04);
+        p = LMD_FMA(p, y, 1.3888888888888889e-03);
+        p = LMD_FMA(p, y, 8.3333333333333332e-03);
+        p = LMD_FMA(p, y, 4.1666666666666664e-02);
+        p = LMD_FMA(p, y, 1.6666666666666666e-01);
+        p = LMD_FMA(p, y, 0.5);
+        p = LMD_FMA(p, y, 1.0);
         return LMD_MUL(p, y);
     }
     return LMD_SUB(lmd_exp_neg(y), 1.0);
@@ -267,18 +274,18 @@ LM_FN double lmd_tanh_pos(double x) {
 LM_FN double lmd_log_series(double s) {
     double s2 = LMD_MUL(s, s);
     double p = 0.040000000000000001;                     /* 1/25 */
-    p = LMD_ADD(LMD_MUL(p, s2), 0.043478260869565216);  /* 1/23 */
-    p = LMD_ADD(LMD_MUL(p, s2), 0.047619047619047616);  /* 1/21 */
-    p = LMD_ADD(LMD_MUL(p, s2), 0.052631578947368418);  /* 1/19 */
-    p = LMD_ADD(LMD_MUL(p, s2), 0.058823529411764705);  /* 1/17 */
-    p = LMD_ADD(LMD_MUL(p, s2), 0.066666666666666666);  /* 1/15 */
-    p = LMD_ADD(LMD_MUL(p, s2), 0.076923076923076927);  /* 1/13 */
-    p = LMD_ADD(LMD_MUL(p, s2), 0.090909090909090912);  /* 1/11 */
-    p = LMD_ADD(LMD_MUL(p, s2), 0.1111111111111111);    /* 1/9 */
-    p = LMD_ADD(LMD_MUL(p, s2), 0.14285714285714285);   /* 1/7 */
-    p = LMD_ADD(LMD_MUL(p, s2), 0.20000000000000001);   /* 1/5 */
-    p = LMD_ADD(LMD_MUL(p, s2), 0.33333333333333331);   /* 1/3 */
-    p = LMD_ADD(LMD_MUL(p, s2), 1.0);
+    p = LMD_FMA(p, s2, 0.043478260869565216);  /* 1/23 */
+    p = LMD_FMA(p, s2, 0.047619047619047616);  /* 1/21 */
+    p = LMD_FMA(p, s2, 0.052631578947368418);  /* 1/19 */
+    p = LMD_FMA(p, s2, 0.058823529411764705);  /* 1/17 */
+    p = LMD_FMA(p, s2, 0.066666666666666666);  /* 1/15 */
+    p = LMD_FMA(p, s2, 0.076923076923076927);  /* 1/13 */
+    p = LMD_FMA(p, s2, 0.090909090909090912);  /* 1/11 */
+    p = LMD_FMA(p, s2, 0.1111111111111111);    /* 1/9 */
+    p = LMD_FMA(p, s2, 0.14285714285714285);   /* 1/7 */
+    p = LMD_FMA(p, s2, 0.20000000000000001);   /* 1/5 */
+    p = LMD_FMA(p, s2, 0.33333333333333331);   /* 1/3 */
+    p = LMD_FMA(p, s2, 1.0);
     return LMD_MUL(2.0, LMD_MUL(p, s));
 }
 
@@ -293,8 +300,8 @@ LM_FN double lmd_log1p_pos(double t) {
     double s = LMD_DIV(LMD_SUB(f, 1.0), LMD_ADD(f, 1.0));
     double ef = (double)e;
     double corr = LMD_DIV(LMD_SUB(t, LMD_SUB(u, 1.0)), u);
-    double lo = LMD_ADD(LMD_ADD(LMD_MUL(ef, LMD_LN2_LO), lmd_log_series(s)), corr);
-    return LMD_ADD(LMD_MUL(ef, LMD_LN2_HI), lo);
+    double lo = LMD_ADD(LMD_FMA(ef, LMD_LN2_LO, lmd_log_series(s)), corr);
+    return LMD_FMA(ef, LMD_LN2_HI, lo);
 }
 
 /* atanh(m) for 0 <= m < 1 */
