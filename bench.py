@@ -308,7 +308,8 @@ def run_workload(args):
     elif args.workload == "hetero-mix":
         out = workloads.hetero_mix(steps=args.steps, warmup=args.warmup)
     elif args.workload == "sp-sweep":
-        out = workloads.sp_sweep(cw_per_z=args.sp_cw, steps=args.steps, warmup=args.warmup)
+        out = workloads.sp_sweep(cw_per_z=args.sp_cw, steps=args.steps, warmup=args.warmup,
+                                 autotune=not args.no_autotune)
     elif args.workload == "variants":
         out = run_variants(args, clk)
     else:

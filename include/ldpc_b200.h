@@ -196,7 +196,8 @@ int ldpc_decode_set_compat(ldpc_ctx *ctx, void *decoded_metrics, unsigned num_co
  * launch is one persistent kernel over all jobs -- for int8 plans, one per
  * geometry class: jobs whose codes would run at different occupancies get
  * separate launches -- and it can be replayed from a CUDA graph (one kernel
- * node per class, free to overlap).  Per codeword, the results are exactly
+ * node per class, free to overlap).  CTAs claim chunks from a per-launch
+ * counter, so a plan's launches on different streams must not overlap.  Per codeword, the results are exactly
  * those of ldpc_decode_int8 / ldpc_decode_count on that code. */
 typedef struct ldpc_batch ldpc_batch;
 typedef struct ldpc_batch_plan ldpc_batch_plan;
@@ -233,10 +234,13 @@ int ldpc_batch_plan_launch(ldpc_batch_plan *p, void *stream);
  * it, ordered after the work already on `stream`. */
 int ldpc_batch_plan_graph_launch(ldpc_batch_plan *p, void *stream);
 void ldpc_batch_plan_destroy(ldpc_batch_plan *p);
+/* Kernels one launch of the plan runs (one per geometry class; 0 when it
+ * has no work). */
+int ldpc_batch_plan_kernels(const ldpc_batch_plan *p);
 
 /* Project autotuner: times plans over the first `sample` codewords of each
  * job (outputs not written) for every CTA width in {128..512} that fits and
- * 1, 2 or 4 chunks per CTA.  It keeps the fastest setting for later plans
+ * 1, 2, 4 or 8 chunks per CTA.  It keeps the fastest setting for later plans
  * and reports it (any output pointer may be NULL).  int8 jobs of several
  * geometry classes: each class is tuned on its own jobs, and that set is
  * kept when it beats the best single shape on the whole sample; the report

@@ -39,6 +39,7 @@ struct ldpc_batch_plan {
     void* d_jobs = nullptr;
     ldpc::RtChunk* d_chunks = nullptr;
     void* d_scratch = nullptr;
+    unsigned int* d_claim = nullptr;        // chunk-claim counter, zeroed before each launch
     cudaStream_t own = nullptr;              // graph capture and replay stream
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     cudaGraph_t graph = nullptr;
@@ -62,9 +63,12 @@ const SpbVariant kSpb[] = {SPB(8, true, true),   SPB(8, true, false),   SPB(8, f
                            SPB(32, true, true),  SPB(32, true, false),  SPB(32, false, true),  SPB(32, false, false)};
 #undef SPB
 
-void launch_plan_kernel(ldpc_batch_plan* p, cudaStream_t s) {
+cudaError_t launch_plan_kernel(ldpc_batch_plan* p, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(p->d_claim, 0, sizeof(unsigned int), s);
+    if (e != cudaSuccess) return e;
     if (p->is_float) ((spb_fn)p->kf)<<<p->grid, p->threads, p->smem, s>>>(p->slp);
     else p->k<<<p->grid, p->threads, p->smem, s>>>(p->lp);
+    return cudaGetLastError();
 }
 
 // Chunks of about equal work (codewords x edges per codeword) so that the
@@ -122,6 +126,7 @@ void release(ldpc_batch_plan* p) {
     cudaFree(p->d_jobs);
     cudaFree(p->d_chunks);
     cudaFree(p->d_scratch);
+    cudaFree(p->d_claim);
 }
 
 struct PlanDel {
@@ -131,11 +136,14 @@ struct PlanDel {
 int float_plan(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int threads, int cpc, ldpc_batch_plan** out) {
     const int nc = (int)b->codes.size();
     const bool prod = b->variant == LDPC_F32_SP;
+    std::vector<char> used(nc, 0);
+    for (int i = 0; i < n_jobs; ++i) used[jobs[i].code] = 1;
     std::vector<int> G(nc, 1);
-    std::vector<size_t> base(nc);
+    std::vector<size_t> base(nc, 0);
     int dmax = 8, maxE = 0;
-    bool rsmem = true;
+    bool rsmem = !getenv("LDPC_SP_RGLOBAL");
     for (int c = 0; c < nc; ++c) {
+        if (!used[c]) continue;
         const ldpc_code& cd = b->codes[c];
         const int n = cd.z * cd.mcol, E = (int)cd.row_cols.size();
         auto bytes = [&](int g) {
@@ -152,11 +160,30 @@ int float_plan(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int thread
         dmax = std::max(dmax, cd.max_row_weight <= 8 ? 8 : cd.max_row_weight <= 16 ? 16 : 32);
         maxE = std::max(maxE, E);
     }
-    size_t smem = 0;
-    for (int c = 0; c < nc; ++c) smem = std::max(smem, base[c] + (rsmem ? (size_t)b->codes[c].row_cols.size() * threads * 4 : 0));
-    spb_fn k = nullptr;
-    for (const SpbVariant& v : kSpb)
-        if (v.dmax == dmax && v.prod == prod && v.rsmem == rsmem) k = v.k;
+    auto find = [&](bool rs) {
+        spb_fn f = nullptr;
+        for (const SpbVariant& v : kSpb)
+            if (v.dmax == dmax && v.prod == prod && v.rsmem == rs) f = v.k;
+        return f;
+    };
+    auto smem_of = [&](bool rs) {
+        size_t m = 0;
+        for (int c = 0; c < nc; ++c)
+            if (used[c]) m = std::max(m, base[c] + (rs ? (size_t)b->codes[c].row_cols.size() * threads * 4 : 0));
+        return m;
+    };
+    if (rsmem && prod) {
+        // as for a single code: sum-product keeps shared-memory messages only
+        // when they keep as many CTAs per SM as global (L2) messages
+        int per_s = 0, per_g = 0;
+        CUDA_TRY(ldpc::allow_dynamic_smem((const void*)find(true), ldpc::kSpMaxSmem));
+        CUDA_TRY(ldpc::allow_dynamic_smem((const void*)find(false), ldpc::kSpMaxSmem));
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_s, (const void*)find(true), threads, smem_of(true)));
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_g, (const void*)find(false), threads, smem_of(false)));
+        rsmem = per_s >= per_g;
+    }
+    const size_t smem = smem_of(rsmem);
+    spb_fn k = find(rsmem);
     std::unique_ptr<ldpc_batch_plan, PlanDel> p(new ldpc_batch_plan);
     p->device = b->device;
     p->is_float = true;
@@ -226,6 +253,8 @@ int float_plan(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int thread
     p->slp.n_chunks = p->d_jobs ? n_chunks : 0;
     p->slp.r_scratch = (float*)p->d_scratch;
     p->slp.r_words_per_cta = words;
+    CUDA_TRY(cudaMalloc(&p->d_claim, sizeof(unsigned int)));
+    p->slp.claim = p->d_claim;
     p->n_chunks = p->slp.n_chunks;
     *out = p.release();
     return LDPC_OK;
@@ -327,22 +356,25 @@ int int8_plan(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int threads
     p->lp.n_chunks = n_chunks;
     p->lp.r_scratch = (uint32_t*)p->d_scratch;
     p->lp.r_words_per_cta = words;
+    CUDA_TRY(cudaMalloc(&p->d_claim, sizeof(unsigned int)));
+    p->lp.claim = p->d_claim;
     if (!p->d_jobs) p->lp.n_chunks = 0;
     p->n_chunks = p->lp.n_chunks;
     *out = p.release();
     return LDPC_OK;
 }
 
-// Occupancy class of a code decoded alone at `threads`: kernel variant,
-// message placement and CTAs per SM.
-struct Int8Class {
+// Class of a code decoded alone at `threads`.  int8: kernel variant,
+// message placement and CTAs per SM.  Float: the width and the row-weight
+// bucket (the float kernel picks its message placement per launch).
+struct PlanClass {
     int dmax = 0, quirk = 0, rsmem = 0, per_sm = 0, threads = 0;
-    bool operator==(const Int8Class& o) const {
+    bool operator==(const PlanClass& o) const {
         return dmax == o.dmax && quirk == o.quirk && rsmem == o.rsmem && per_sm == o.per_sm && threads == o.threads;
     }
 };
 
-int int8_class(const ldpc_batch* b, int c, int threads, Int8Class* out) {
+int int8_class(const ldpc_batch* b, int c, int threads, PlanClass* out) {
     const ldpc_code& cd = b->codes[c];
     const int n = cd.z * cd.mcol, E = (int)cd.row_cols.size();
     int G = std::max(1, std::min(16, threads / cd.z));
@@ -364,26 +396,42 @@ int int8_class(const ldpc_batch* b, int c, int threads, Int8Class* out) {
     return LDPC_OK;
 }
 
-// Class index of every code used by the jobs (code_cls[c], -1 if unused);
-// returns the number of classes.  Widths: `threads` when explicit, else each
-// code's default max(256, Z rounded to 32).
-int int8_classes(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, bool explicit_threads, int threads,
-                 std::vector<int>& code_cls, int* n_cls) {
+// A code's own CTA width: int8 max(256, Z rounded to 32); float the
+// single-code context's G*Z rounded to 32, G = 128 / Z codewords per CTA.
+int default_width(const ldpc_batch* b, int z) {
+    if (b->variant == LDPC_INT8_OMS) return std::max(256, ((z + 31) / 32) * 32);
+    const int G = std::max(1, std::min(32, 128 / z));
+    return std::min(ldpc::kRtMaxThreads, ((G * z + 31) / 32) * 32);
+}
+
+// Class index of every code used by the jobs (code_cls[c], -1 if unused)
+// and each class's width; returns the number of classes.  Widths: `threads`
+// when explicit, else each code's own width.
+int plan_classes(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, bool explicit_threads, int threads,
+                 std::vector<int>& code_cls, std::vector<int>& cls_threads, int* n_cls) {
     const int nc = (int)b->codes.size();
-    std::vector<Int8Class> cls;
+    std::vector<PlanClass> cls;
     code_cls.assign(nc, -1);
+    cls_threads.clear();
     for (int i = 0; i < n_jobs; ++i) {
         const int c = jobs[i].code;
         if (code_cls[c] >= 0) continue;
-        Int8Class k;
-        const int t = explicit_threads ? threads : std::max(256, ((b->codes[c].z + 31) / 32) * 32);
-        if (int rc = int8_class(b, c, t, &k)) return rc;
+        PlanClass k;
+        const int t = explicit_threads ? threads : default_width(b, b->codes[c].z);
+        if (b->variant == LDPC_INT8_OMS) {
+            if (int rc = int8_class(b, c, t, &k)) return rc;
+        } else {
+            const int w = b->codes[c].max_row_weight;
+            k.dmax = w <= 8 ? 8 : w <= 16 ? 16 : 32;
+            k.threads = t;
+        }
         int idx = -1;
         for (size_t j = 0; j < cls.size(); ++j)
             if (cls[j] == k) idx = (int)j;
         if (idx < 0) {
             idx = (int)cls.size();
             cls.push_back(k);
+            cls_threads.push_back(t);
         }
         code_cls[c] = idx;
     }
@@ -404,31 +452,39 @@ std::vector<ldpc_batch_job> class_jobs(const ldpc_batch* b, const ldpc_batch_job
     return sub;
 }
 
-// The jobs grouped by the occupancy class of their code; one launch per
-// class (a single launch when there is one class, or when LDPC_BATCH_ONE_LAUNCH
-// is set).  threads: the caller's width, applied to every class when
-// explicit; otherwise each class takes its tuned shape (ldpc_batch_autotune)
-// or max(256, its largest Z rounded to 32) and `cpc`.
-int int8_plan_classes(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, bool explicit_threads, int threads,
-                      int cpc, ldpc_batch_plan** out) {
-    if (getenv("LDPC_BATCH_ONE_LAUNCH") || n_jobs < 2) return int8_plan(b, jobs, n_jobs, threads, cpc, out);
-    std::vector<int> code_cls;
+int one_plan(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int threads, int cpc, ldpc_batch_plan** out) {
+    return b->variant == LDPC_INT8_OMS ? int8_plan(b, jobs, n_jobs, threads, cpc, out)
+                                       : float_plan(b, jobs, n_jobs, threads, cpc, out);
+}
+
+// The jobs grouped by the class of their code; one launch per class (a
+// single launch when there is one class, or when LDPC_BATCH_ONE_LAUNCH is
+// set).  threads: the caller's width, applied to every class when explicit;
+// otherwise each class takes its tuned shape (ldpc_batch_autotune) or its
+// codes' own width and `cpc`.
+int plans_by_class(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, bool explicit_threads, int threads,
+                   int cpc, ldpc_batch_plan** out) {
+    if (getenv("LDPC_BATCH_ONE_LAUNCH") || n_jobs < 2) return one_plan(b, jobs, n_jobs, threads, cpc, out);
+    std::vector<int> code_cls, cls_threads;
     int n_cls = 0;
-    if (int rc = int8_classes(b, jobs, n_jobs, explicit_threads, threads, code_cls, &n_cls)) return rc;
-    if (n_cls < 2) return int8_plan(b, jobs, n_jobs, threads, cpc, out);
+    if (int rc = plan_classes(b, jobs, n_jobs, explicit_threads, threads, code_cls, cls_threads, &n_cls)) return rc;
+    if (n_cls < 2) {
+        if (!explicit_threads && n_cls == 1) threads = cls_threads[0];
+        return one_plan(b, jobs, n_jobs, threads, cpc, out);
+    }
     std::unique_ptr<ldpc_batch_plan, PlanDel> p(new ldpc_batch_plan);
     p->device = b->device;
     for (int k = 0; k < n_cls; ++k) {
         int maxz = 0;
         std::vector<ldpc_batch_job> sub = class_jobs(b, jobs, n_jobs, code_cls, k, &maxz);
-        int t = explicit_threads ? threads : std::max(256, ((maxz + 31) / 32) * 32);
+        int t = explicit_threads ? threads : cls_threads[k];
         int c = cpc;
         if (!explicit_threads && !b->code_threads.empty() && b->code_threads[sub[0].code] >= maxz) {
             t = b->code_threads[sub[0].code];
             c = b->code_cpc[sub[0].code];
         }
         ldpc_batch_plan* part = nullptr;
-        if (int rc = int8_plan(b, sub.data(), (int)sub.size(), t, c, &part)) return rc;
+        if (int rc = one_plan(b, sub.data(), (int)sub.size(), t, c, &part)) return rc;
         p->parts.push_back(part);
         p->n_chunks += part->n_chunks;
     }
@@ -522,8 +578,7 @@ int ldpc_batch_plan_create(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs
     if (threads % 32 || threads > ldpc::kRtMaxThreads || threads < maxz)
         return fail(LDPC_ERR_UNSUPPORTED, "batch plan: %d threads per CTA (multiple of 32, >= Z=%d, <= %d)", threads, maxz,
                     ldpc::kRtMaxThreads);
-    if (b->variant != LDPC_INT8_OMS) return float_plan(b, jobs, n_jobs, threads, cpc, out);
-    return int8_plan_classes(b, jobs, n_jobs, explicit_threads, threads, cpc, out);
+    return plans_by_class(b, jobs, n_jobs, explicit_threads, threads, cpc, out);
 }
 
 int ldpc_batch_plan_launch(ldpc_batch_plan* p, void* stream) {
@@ -531,12 +586,11 @@ int ldpc_batch_plan_launch(ldpc_batch_plan* p, void* stream) {
     if (p->n_chunks == 0) return LDPC_OK;
     CUDA_TRY(cudaSetDevice(p->device));
     if (p->parts.empty()) {
-        launch_plan_kernel(p, (cudaStream_t)stream);
+        CUDA_TRY(launch_plan_kernel(p, (cudaStream_t)stream));
     } else {
         for (ldpc_batch_plan* q : p->parts)
-            if (q->n_chunks) launch_plan_kernel(q, (cudaStream_t)stream);
+            if (q->n_chunks) CUDA_TRY(launch_plan_kernel(q, (cudaStream_t)stream));
     }
-    CUDA_TRY(cudaGetLastError());
     return LDPC_OK;
 }
 
@@ -548,8 +602,9 @@ int ldpc_batch_plan_graph_launch(ldpc_batch_plan* p, void* stream) {
         if (!p->own) CUDA_TRY(cudaStreamCreateWithFlags(&p->own, cudaStreamNonBlocking));
         if (!p->ev_in) CUDA_TRY(cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming));
         if (!p->ev_out) CUDA_TRY(cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming));
-        // one kernel node per launch of the plan, with no edges between them:
-        // the per-class launches may run side by side
+        // per launch of the plan: a memset node (its chunk-claim counter)
+        // then its kernel node; no edges between launches, so the per-class
+        // launches may run side by side
         cudaGraph_t g = nullptr;
         CUDA_TRY(cudaGraphCreate(&g, 0));
         std::vector<ldpc_batch_plan*> leaves = p->parts;
@@ -565,8 +620,16 @@ int ldpc_batch_plan_graph_launch(ldpc_batch_plan* p, void* stream) {
             kp.blockDim = dim3((unsigned)q->threads);
             kp.sharedMemBytes = (unsigned)q->smem;
             kp.kernelParams = &arg;
-            cudaGraphNode_t node;
-            if ((e = cudaGraphAddKernelNode(&node, g, nullptr, 0, &kp)) != cudaSuccess) break;
+            cudaMemsetParams mp;
+            memset(&mp, 0, sizeof(mp));
+            mp.dst = q->d_claim;
+            mp.value = 0;
+            mp.elementSize = sizeof(unsigned int);
+            mp.width = 1;
+            mp.height = 1;
+            cudaGraphNode_t mnode, node;
+            if ((e = cudaGraphAddMemsetNode(&mnode, g, nullptr, 0, &mp)) != cudaSuccess) break;
+            if ((e = cudaGraphAddKernelNode(&node, g, &mnode, 1, &kp)) != cudaSuccess) break;
         }
         if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, g, 0);
         if (e != cudaSuccess) {
@@ -586,6 +649,14 @@ int ldpc_batch_plan_graph_launch(ldpc_batch_plan* p, void* stream) {
 }
 
 void ldpc_batch_plan_destroy(ldpc_batch_plan* p) { PlanDel()(p); }
+
+int ldpc_batch_plan_kernels(const ldpc_batch_plan* p) {
+    if (!p || p->n_chunks == 0) return 0;
+    if (p->parts.empty()) return 1;
+    int k = 0;
+    for (const ldpc_batch_plan* q : p->parts) k += q->n_chunks ? 1 : 0;
+    return k;
+}
 
 }  // extern "C"
 
@@ -615,12 +686,12 @@ int time_shape(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int t, int
 }
 
 // The fastest (width, chunks per CTA) for these jobs: every width of
-// kTunedWidths >= maxz and 1, 2 or 4 chunks per CTA.
+// kTunedWidths >= maxz and 1, 2, 4 or 8 chunks per CTA.
 int tune_shape(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int maxz, cudaStream_t s, cudaEvent_t e0,
                cudaEvent_t e1, int* t_out, int* c_out, double* ms_out) {
     double best = 1e30;
     int best_t = 0, best_c = 0;
-    const int cpcs[] = {1, 2, 4};
+    const int cpcs[] = {1, 2, 4, 8};
     for (int t : kTunedWidths) {
         if (t < maxz) continue;
         for (int c : cpcs) {
@@ -667,14 +738,14 @@ int ldpc_batch_autotune(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, s
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));
     int rc = LDPC_OK;
-    std::vector<int> code_cls;
+    std::vector<int> code_cls, cls_threads;
     int n_cls = 1;
-    if (b->variant == LDPC_INT8_OMS && !getenv("LDPC_BATCH_ONE_LAUNCH") && n_jobs > 1)
-        rc = int8_classes(b, sj.data(), n_jobs, false, 0, code_cls, &n_cls);
+    if (!getenv("LDPC_BATCH_ONE_LAUNCH") && n_jobs > 1)
+        rc = plan_classes(b, sj.data(), n_jobs, false, 0, code_cls, cls_threads, &n_cls);
     double best = 1e30, worst = -1;
     int best_t = 0, best_c = 0;
     if (rc == LDPC_OK && n_cls > 1) {
-        // int8 classes: each class is its own launch.  Candidates: every class
+        // several classes: each class is its own launch.  Candidates: every class
         // tuned on its own jobs, and one shape for all classes; the whole
         // sample plan decides between them.
         std::vector<int> ct(b->codes.size(), 0), cc(b->codes.size(), 0);

@@ -79,10 +79,33 @@ int setup_sp(ldpc_ctx* x) {
     t.nostage = nostage ? 1 : 0;
     x->sp_threads = ((G * c.z + 31) / 32) * 32;
     const size_t r_smem = (size_t)t.E * x->sp_threads * es;
-    const bool rsmem = base_smem + r_smem <= 160 * 1024;
-    const SpVariant* v = nullptr;
-    for (const SpVariant& k : kSp)
-        if (k.dmax == dmax && k.prod == prod && k.rsmem == rsmem) v = &k;
+    // sum-product: messages in shared memory only when that keeps as many
+    // CTAs per SM as messages in global scratch (L2) would -- its tanh/atanh
+    // chains are latency-bound, so resident warps count for more than
+    // message latency.  Min-sum, light on arithmetic, keeps them in shared
+    // memory whenever they fit.
+    auto find = [&](bool rs) {
+        const SpVariant* f = nullptr;
+        for (const SpVariant& k : kSp)
+            if (k.dmax == dmax && k.prod == prod && k.rsmem == rs) f = &k;
+        return f;
+    };
+    auto ctas_per_sm = [&](const SpVariant* k, size_t bytes, int* out) -> cudaError_t {
+        const void* fn = dbl ? (const void*)k->k64 : (const void*)k->k;
+        cudaError_t e = allow_dynamic_smem(fn, kSpMaxSmem);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, fn, x->sp_threads, bytes);
+        return e;
+    };
+    // tuning: LDPC_SP_RGLOBAL forces global messages, LDPC_SP_RSMEM shared
+    // ones where they fit
+    bool rsmem = false;
+    if (base_smem + r_smem <= 160 * 1024 && !getenv("LDPC_SP_RGLOBAL")) {
+        int per_s = 0, per_g = 0;
+        CUDA_TRY(ctas_per_sm(find(true), base_smem + r_smem, &per_s));
+        CUDA_TRY(ctas_per_sm(find(false), base_smem, &per_g));
+        rsmem = !prod || per_s >= per_g || getenv("LDPC_SP_RSMEM");
+    }
+    const SpVariant* v = find(rsmem);
     x->sp_kernel = dbl ? nullptr : v->k;
     x->sp64_kernel = dbl ? v->k64 : nullptr;
     const void* kfn = dbl ? (const void*)v->k64 : (const void*)v->k;

@@ -144,7 +144,17 @@ __global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtL
     if (tid == 0) s_code_idx = -1;
 
     const int n_chunks = lp.jobs ? lp.n_chunks : (int)gridDim.x;
-    for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
+    __shared__ int s_claim;
+    // chunk b first, then the next unclaimed chunk (batch plans) or chunk
+    // b + grid: CTAs that drew cheap chunks take more of them
+    auto next_chunk = [&](int ci) -> int {
+        if (!lp.claim) return ci + (int)gridDim.x;
+        __syncthreads();
+        if (tid == 0) s_claim = (int)gridDim.x + (int)atomicAdd(lp.claim, 1u);
+        __syncthreads();
+        return s_claim;
+    };
+    for (int ci = blockIdx.x; ci < n_chunks; ci = next_chunk(ci)) {
         // ---------------- chunk set-up ----------------
         RtJob job;
         long long lo, hi;

@@ -34,6 +34,7 @@ struct SpBatchLaunch {
     const SpBatchJob* jobs;
     const RtChunk* chunks;
     int n_chunks;
+    unsigned int* claim;             // chunks claimed beyond the first grid (zeroed before each launch)
     float* r_scratch;                // per-CTA messages when they do not fit shared memory
     long long r_words_per_cta;
 };
@@ -47,7 +48,17 @@ __global__ void __launch_bounds__(512) sp_batch_kernel(const __grid_constant__ S
     const SpCode& C = *reinterpret_cast<const SpCode*>(spb_smem);
     float* sm_f = reinterpret_cast<float*>(spb_smem + sp_code_bytes());
     if (threadIdx.x == 0) s_code = -1;
-    for (int ci = blockIdx.x; ci < lp.n_chunks; ci += gridDim.x) {
+    __shared__ int s_claim;
+    // chunk b first, then the next unclaimed chunk: CTAs that drew cheap
+    // chunks take more of them
+    auto next_chunk = [&](int ci) -> int {
+        if (!lp.claim) return ci + (int)gridDim.x;
+        __syncthreads();
+        if (threadIdx.x == 0) s_claim = (int)gridDim.x + (int)atomicAdd(lp.claim, 1u);
+        __syncthreads();
+        return s_claim;
+    };
+    for (int ci = blockIdx.x; ci < lp.n_chunks; ci = next_chunk(ci)) {
         const RtChunk ch = lp.chunks[ci];
         const SpBatchJob bj = lp.jobs[ch.job];
         __syncthreads();   // the previous chunk is finished with the shared tables and state

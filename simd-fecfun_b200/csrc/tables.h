@@ -120,8 +120,9 @@ struct RtChunk {
 struct RtLaunch {
     const RtCode* codes;
     const RtJob* jobs;               // null: one job, job0, split evenly over the grid
-    const RtChunk* chunks;           // CTA b takes chunks b, b + grid, b + 2 grid, ...
+    const RtChunk* chunks;           // CTA b takes chunk b first, then the next claimed one (or b + grid, ...)
     int n_chunks;
+    unsigned int* claim;             // chunks claimed beyond the first grid (zeroed before each launch), or null
     RtJob job0;
     uint32_t* r_scratch;             // check messages in global memory (when not in shared memory)
     long long r_words_per_cta;

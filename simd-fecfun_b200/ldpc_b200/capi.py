@@ -103,6 +103,7 @@ _PROTOS = {
     "ldpc_batch_plan_launch": (C.c_int, [_vp, _vp]),
     "ldpc_batch_plan_graph_launch": (C.c_int, [_vp, _vp]),
     "ldpc_batch_plan_destroy": (None, [_vp]),
+    "ldpc_batch_plan_kernels": (C.c_int, [_vp]),
     "ldpc_learned_grid": (C.c_int, [_vp, _sz, C.POINTER(C.c_int)]),
     "ldpc_learned_forward": (C.c_int, [_vp, _vp, _sz, C.c_int, _vp, _vp, _vp, _vp]),
     "ldpc_learned_backward": (C.c_int, [_vp, _sz, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_float, _vp, _vp, _vp]),
@@ -373,6 +374,11 @@ class BatchPlan:
 
     def graph_launch(self, stream=0):
         check(lib.ldpc_batch_plan_graph_launch(self.h, stream or None))
+
+    @property
+    def kernels(self) -> int:
+        """Kernels one launch runs (one per geometry class)."""
+        return int(lib.ldpc_batch_plan_kernels(self.h))
 
     def close(self):
         if getattr(self, "h", None):

@@ -140,14 +140,15 @@ def nr_mix(steps: int = 3, warmup: int = 1, seed: int = 7, llr_budget: float = 4
                                % (", ".join(names), counts,
                                   "" if scale >= 1 else ", scaled by %.3f to fit %.0f GB of LLRs" % (scale, llr_budget / 1e9),
                                   list(ebn0)),
-                   "launch": "one persistent kernel over %d jobs, replayed from a CUDA graph" % len(specs),
+                   "launch": "%d persistent kernels (one per geometry class) over %d jobs, in one CUDA graph"
+                             % (plan.kernels, len(specs)),
                    "autotuned": {"threads": tuned[0], "chunks_per_cta": tuned[1], "sample_ms": tuned[2],
                                  "tuning_s": round(tune_s, 2)},
                    "l2": "inputs larger than L2 (%.1f GB of LLRs)" % (sum(m * c.n for m, c in zip(counts, objs)) / 1e9)},
         "info_gbps": info_bits / (avg_ms * 1e-3) / 1e9,
         "per_code_sequential": {"value": total / (seq_ms * 1e-3), "unit": "codewords/s",
                                 "note": "same jobs, one ldpc_decode_count launch per job"},
-        "gpu_launches": steps,
+        "gpu_launches": steps * plan.kernels,
         "quality": quality,
     }
 
@@ -217,10 +218,11 @@ def hetero_mix(steps: int = 3, warmup: int = 1, total: int = 10_000_000, seed: i
         "value": total / (avg_plain * 1e-3), "unit": "codewords/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
         "ms_per_step": avg_plain, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
         "data": "synthetic: Philox data bits, QC encoding, AWGN from the fused generator, resident in HBM",
-        "config": {"workload": "%d codes (%s), %d codewords in one persistent launch (equal split), per-code SNR "
+        "config": {"workload": "%d codes (%s), %d codewords in one CUDA graph (equal split), per-code SNR "
                                "calibrated to CWER 1e-3 (bisection over ldpc_simulate, 1e5 codewords per point, %.1f s)"
                                % (len(names), ", ".join(names), total, cal_s),
                    "autotuned": {"threads": tuned[0], "chunks_per_cta": tuned[1]},
+                   "launch": "%d persistent kernels (one per geometry class) in one CUDA graph" % plan.kernels,
                    "snr_db": dict(zip(names, [round(s, 3) for s in snr]))},
         "info_gbps": sum(m * c.k for m, c in zip(counts, objs)) / (avg_plain * 1e-3) / 1e9,
         "learned": {"value": total / (avg_learned * 1e-3), "unit": "codewords/s", "avg_iter": it_l,
@@ -229,7 +231,7 @@ def hetero_mix(steps: int = 3, warmup: int = 1, total: int = 10_000_000, seed: i
                                 "calibrated SNR +-0.25 dB; offsets averaged over iterations, x2 (int8 LLR scale), "
                                 "rounded" % train_steps},
         "plain_avg_iter": it_p,
-        "gpu_launches": steps,
+        "gpu_launches": steps * plan.kernels,
         "quality_plain": q_plain, "quality_learned": q_learned,
     }
 
@@ -296,7 +298,7 @@ def learned_run(train_steps: int = 30, batch: int = 65536, eval_n: int = 200_000
 
 
 def sp_sweep(cw_per_z: int = 1 << 20, ebn0=(0.5, 1.0, 1.5, 2.0), seed: int = 5, max_iter: int = 10,
-             llr_budget: float = 60e9, steps: int = 1, warmup: int = 1) -> Dict:
+             llr_budget: float = 60e9, steps: int = 1, warmup: int = 1, autotune: bool = True) -> Dict:
     """802.16e rate 1/2 for every Z = 24, 28, ..., 96 (N = 576..2304), float
     sum-product (clamp 1 - 6e-8, LLR = 2y/sigma^2, no LLR limit), 10
     iterations.  All 19 codes, their codewords spread over the Eb/N0 points,
@@ -330,7 +332,7 @@ def sp_sweep(cw_per_z: int = 1 << 20, ebn0=(0.5, 1.0, 1.5, 2.0), seed: int = 5, 
     torch.cuda.synchronize()
     batch = capi.Batch(handles, [kw] * len(objs))
     t0 = time.time()
-    tuned = batch.autotune(specs, sample=8192)
+    tuned = batch.autotune(specs, sample=8192) if autotune else (0, 0, 0.0)
     tune_s = time.time() - t0
     plan = batch.plan(specs)
     ms = _time_plan(plan, specs, steps, warmup)
@@ -359,7 +361,8 @@ def sp_sweep(cw_per_z: int = 1 << 20, ebn0=(0.5, 1.0, 1.5, 2.0), seed: int = 5, 
                                "(Es/N0 = Eb/N0 - 3.01 dB), sum-product clamp 1-6e-8, LLR scale 1, no LLR limit"
                                % (per_z, "" if scale >= 1 else " (2^20 scaled by %.3f to fit %.0f GB of float LLRs)"
                                   % (scale, llr_budget / 1e9), list(ebn0)),
-                   "launch": "one persistent float batch kernel over %d jobs, replayed from a CUDA graph" % len(specs),
+                   "launch": "%d persistent float batch kernels (one per geometry class) over %d jobs, in one "
+                             "CUDA graph" % (plan.kernels, len(specs)),
                    "autotuned": {"threads": tuned[0], "chunks_per_cta": tuned[1], "sample_ms": tuned[2],
                                  "tuning_s": round(tune_s, 2)},
                    "l2": "inputs larger than L2 (%.1f GB of LLRs)" % (sum(sp["n"] * objs[sp["code"]].n * 4
@@ -367,7 +370,7 @@ def sp_sweep(cw_per_z: int = 1 << 20, ebn0=(0.5, 1.0, 1.5, 2.0), seed: int = 5, 
         "info_gbps": info_bits / (avg_ms * 1e-3) / 1e9,
         "per_launch_sequential": {"value": total / (seq_ms * 1e-3), "unit": "codewords/s",
                                   "note": "same jobs, one ldpc_decode_count launch per (Z, Eb/N0)"},
-        "gpu_launches": steps,
+        "gpu_launches": steps * plan.kernels,
         "quality": quality,
     }
 

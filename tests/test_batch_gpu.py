@@ -142,7 +142,7 @@ def test_autotune_then_plan(capi, oracle):
     import torch
     batch, objs, handles, data, specs, bufs = _mix(capi, oracle)
     t, c, ms = batch.autotune(specs, sample=256)
-    assert t in (128, 192, 256, 320, 384, 448, 512) and c in (1, 2, 4) and ms > 0
+    assert t in (128, 192, 256, 320, 384, 448, 512) and c in (1, 2, 4, 8) and ms > 0
     plan = batch.plan(specs)      # uses the tuned shape
     _clear(bufs)
     plan.launch()
@@ -214,3 +214,26 @@ def test_batch_variants_must_agree(capi):
     fb = capi.Batch([h], [dict(variant=capi.LDPC_F32_OMS)])
     with pytest.raises(capi.LdpcError):
         fb.set_offsets(0, np.ones(8, np.float32))
+
+
+def test_geometry_classes_and_single_launch(capi, oracle):
+    """Codes of different occupancy classes get one kernel each (graph nodes
+    free to overlap); LDPC_BATCH_ONE_LAUNCH keeps one kernel; the results are
+    the same either way."""
+    import os
+    import torch
+    batch, objs, handles, data, specs, bufs = _mix(capi, oracle)
+    plan = batch.plan(specs)
+    assert plan.kernels >= 2
+    os.environ["LDPC_BATCH_ONE_LAUNCH"] = "1"
+    try:
+        one = batch.plan(specs)
+    finally:
+        os.environ.pop("LDPC_BATCH_ONE_LAUNCH", None)
+    assert one.kernels == 1
+    for p in (plan, one):
+        _clear(bufs)
+        torch.cuda.synchronize()
+        p.graph_launch(torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        _verify(oracle, objs, handles, data, bufs)

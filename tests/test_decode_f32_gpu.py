@@ -51,6 +51,24 @@ def test_float_min_sum_matches_oracle(capi, oracle, name, snr):
     _check(capi, oracle, code, _float_llr(code, 200, snr, 5, oracle), 0, 31.0, 0.5)
 
 
+@pytest.mark.parametrize("env", ["LDPC_SP_RSMEM", "LDPC_SP_RGLOBAL"])
+@pytest.mark.parametrize("mode", [1, 0])
+def test_message_placements(capi, oracle, env, mode):
+    """Check messages in shared memory and in global scratch (the context
+    picks by occupancy; the switches force each placement)."""
+    import os
+    from ldpc_b200 import codes
+    for name, snr in (("16e 1/2", 1.0), ("11ad 1/2", -0.5)):
+        code = codes.make_code(name)
+        os.environ[env] = "1"
+        try:
+            llr = _float_llr(code, 150, snr, 7, oracle)
+            mrm, beta = (6e-8, 0.0) if mode == 1 else (31.0, 0.5)
+            _check(capi, oracle, code, llr, mode, mrm, beta)
+        finally:
+            os.environ.pop(env, None)
+
+
 def test_large_code_messages_in_global_memory(capi, oracle):
     """802.3ca (Z=256, 12 x 69): messages exceed shared memory."""
     from ldpc_b200 import codes
