@@ -9,7 +9,10 @@
   differentiate.
 * :func:`train` / :func:`evaluate` -- training on codewords drawn by the
   library's own generator (Philox data bits, QC encoder, AWGN), and decoding
-  with the learned offsets and early exit.
+  with the learned offsets and early exit.  Under ``torch.distributed``
+  training is data-parallel: every rank draws its own codewords and the
+  offset gradients are averaged over the ranks (:func:`average_gradients`,
+  one all-reduce of iters x layers floats per step).
 
 The decoder is the reference's layered offset min-sum (decode_functions.cpp:
 11-103, float variant) with the single offset ``beta_offset`` (sim_struct_
@@ -146,10 +149,38 @@ def draw(ctx, code, n: int, snr_db: Sequence[float], seed: int, offset: int):
     return torch.cat(llrs), torch.cat(bits)
 
 
+def average_gradients(params, group=None) -> None:
+    """Data-parallel step: replace each gradient by its mean over the ranks
+    of ``group`` (every rank decoded its own, equally sized batch, so this is
+    the gradient of the loss over all ranks' codewords).  No-op without an
+    initialised process group."""
+    dist = torch.distributed
+    if not (dist.is_available() and dist.is_initialized()):
+        return
+    world = dist.get_world_size(group)
+    for p in params:
+        if p.grad is not None:
+            dist.all_reduce(p.grad, op=dist.ReduceOp.SUM, group=group)
+            p.grad /= world
+
+
+def _rank_world(group=None):
+    dist = torch.distributed
+    if dist.is_available() and dist.is_initialized():
+        return dist.get_rank(group), dist.get_world_size(group)
+    return 0, 1
+
+
 def train(ctx, code, iters: int = 10, batch: int = 65536, steps: int = 100, ebn0=(1.0, 2.5), lr: float = 0.01,
-          init: float = 0.5, seed: int = 1, n_snr: int = 16, loss_w: Optional[Sequence[float]] = None, log=None):
+          init: float = 0.5, seed: int = 1, n_snr: int = 16, loss_w: Optional[Sequence[float]] = None, log=None,
+          group=None):
     """Adam on beta [iters][mrow] (initialised to ``init``); every step draws
-    a fresh batch at Eb/N0 points spread uniformly over ``ebn0``."""
+    a fresh batch at Eb/N0 points spread uniformly over ``ebn0``.  With a
+    process group, ``batch`` is per rank: rank r draws codewords
+    [(step * world + r) * batch, ...) of the generator's stream, the ranks
+    share the Eb/N0 draw (same ``seed``) and average their gradients, so
+    their offsets stay identical."""
+    rank, world = _rank_world(group)
     rate = code.k / (code.n - code.punc_cnt_bits - code.fill_cnt)
     beta = torch.full((iters, code.mrow), init, dtype=torch.float32, device="cuda", requires_grad=True)
     w = torch.tensor(loss_w if loss_w is not None else [1.0] * iters, dtype=torch.float32, device="cuda")
@@ -158,10 +189,11 @@ def train(ctx, code, iters: int = 10, batch: int = 65536, steps: int = 100, ebn0
     history = []
     for step in range(steps):
         eb = rng.uniform(ebn0[0], ebn0[1], n_snr)
-        llr, bits = draw(ctx, code, batch, [snr_from_ebn0(e, rate) for e in eb], seed, step * batch)
+        llr, bits = draw(ctx, code, batch, [snr_from_ebn0(e, rate) for e in eb], seed, (step * world + rank) * batch)
         opt.zero_grad()
         loss = LearnedOMSLoss.apply(beta, llr, bits, w, ctx)
         loss.backward()
+        average_gradients([beta], group)
         opt.step()
         with torch.no_grad():
             beta.clamp_(min=0.0)
