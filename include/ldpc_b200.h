@@ -115,6 +115,15 @@ void ldpc_ctx_destroy(ldpc_ctx *ctx);
  * flight. */
 int ldpc_ctx_set_layer_offsets(ldpc_ctx *ctx, const float *beta_per_layer);
 
+/* int8 contexts: an offset table beta[rows][mrow] (1 <= rows <= 255, values
+ * truncated to int8 like cfg.beta): iteration i (0-based) of a codeword uses
+ * row min(i, rows - 1) -- learned per-(iteration, layer) offsets quantised to
+ * the int8 LLR scale.  NULL restores cfg.beta; a later
+ * ldpc_ctx_set_layer_offsets replaces it.  The reference applies one offset
+ * everywhere (decode_functions.cpp:59-62).  Decoding runs on the
+ * run-time-table kernel; the call waits for the device to be idle. */
+int ldpc_ctx_set_offset_table(ldpc_ctx *ctx, const float *beta, unsigned rows);
+
 /* ---- decoding ------------------------------------------------------------- */
 
 /* Decode n codewords of int8 LLRs (variant LDPC_INT8_OMS).  Replaces
@@ -222,6 +231,10 @@ int ldpc_batch_create(const ldpc_code *const *codes, const ldpc_cfg *cfgs, int n
  * 0..127).  NULL restores cfg.beta on every layer.  It affects plans
  * created afterwards. */
 int ldpc_batch_set_offsets(ldpc_batch *b, int code, const float *beta_per_layer);
+/* An offset table beta[rows][mrow] for code `code` (as
+ * ldpc_ctx_set_offset_table); NULL restores cfg.beta.  It replaces the
+ * code's per-layer offsets and affects plans created afterwards. */
+int ldpc_batch_set_offset_table(ldpc_batch *b, int code, const float *beta, unsigned rows);
 void ldpc_batch_destroy(ldpc_batch *b);
 
 /* Plan over `jobs`.  threads = CTA width, for every class (0: the autotuned

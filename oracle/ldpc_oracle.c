@@ -72,8 +72,12 @@ static const orc_trees *g_trees_i8 = 0;
 /* int8 layered offset min-sum with offset beta8[r] on layer r (the
  * reference's decoder has one offset for every layer; per-layer offsets are
  * the learned-offset extension). */
-int orc_decode_int8_layers(const orc_code *c, const int8_t *llr, size_t n_cw, unsigned max_iter,
-                           float max_row_metric, const int8_t *beta_layer, int8_t *post_out, uint32_t *iters_out) {
+/* int8 decoding with an offset table beta_tab[rows][mrow]: iteration i
+ * (0-based) of a codeword uses row min(i, rows - 1).  One row is one offset
+ * per layer; the reference's single beta is one row of equal values. */
+int orc_decode_int8_table(const orc_code *c, const int8_t *llr, size_t n_cw, unsigned max_iter,
+                          float max_row_metric, const int8_t *beta_tab, int rows, int8_t *post_out,
+                          uint32_t *iters_out) {
     const int z = c->z, n = z * c->mcol, E = total_edges(c), dmax = max_weight(c);
     const int8_t maxv = max_row_i8(max_row_metric);
     int8_t *P = (int8_t *)malloc((size_t)n);
@@ -90,7 +94,8 @@ int orc_decode_int8_layers(const orc_code *c, const int8_t *llr, size_t n_cw, un
             int e0 = 0;
             for (int r = 0; r < c->mrow; ++r) {
                 const int d = c->row_weights[r];
-                const int8_t beta8 = beta_layer[r];
+                const int row = (int)iter < rows ? (int)iter : rows - 1;
+                const int8_t beta8 = beta_tab[(size_t)row * c->mrow + r];
                 for (int t = 0; t < z; ++t) {
                     int8_t rx = 0;
                     for (int j = 0; j < d; ++j) {
@@ -139,6 +144,11 @@ int orc_decode_int8_layers(const orc_code *c, const int8_t *llr, size_t n_cw, un
     }
     free(P); free(R); free(Q); free(m); free(f); free(node); free(v);
     return 0;
+}
+
+int orc_decode_int8_layers(const orc_code *c, const int8_t *llr, size_t n_cw, unsigned max_iter,
+                           float max_row_metric, const int8_t *beta_layer, int8_t *post_out, uint32_t *iters_out) {
+    return orc_decode_int8_table(c, llr, n_cw, max_iter, max_row_metric, beta_layer, 1, post_out, iters_out);
 }
 
 int orc_decode_int8(const orc_code *c, const int8_t *llr, size_t n_cw, unsigned max_iter,

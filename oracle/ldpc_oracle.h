@@ -35,6 +35,11 @@ typedef struct {
     int max_d;
 } orc_trees;
 
+/* orc_decode_int8 with an offset table beta_tab[rows][mrow] (int8):
+ * iteration i of a codeword uses row min(i, rows - 1) */
+int orc_decode_int8_table(const orc_code *c, const int8_t *llr, size_t n_cw, unsigned max_iter,
+                          float max_row_metric, const int8_t *beta_tab, int rows, int8_t *post_out,
+                          uint32_t *iters_out);
 /* orc_decode_int8 with one offset per layer (beta_layer[mrow], int8) */
 int orc_decode_int8_layers(const orc_code *c, const int8_t *llr, size_t n_cw, unsigned max_iter,
                            float max_row_metric, const int8_t *beta_layer, int8_t *post_out, uint32_t *iters_out);

@@ -197,14 +197,24 @@ class Oracle:
                                        keep[2].ctypes.data_as(p), 53), keep)
         return self._trees[0]
 
-    def decode_int8(self, code, llr, max_iter=10, max_row_metric=31.0, beta=1.0, use_tree=False, beta_layers=None):
+    def decode_int8(self, code, llr, max_iter=10, max_row_metric=31.0, beta=1.0, use_tree=False, beta_layers=None,
+                    beta_table=None):
         """int8 layered offset min-sum; ``beta_layers`` (one int8 offset per
-        layer) replaces the single ``beta``."""
+        layer) or ``beta_table`` ([rows][layers] int8, iteration i uses row
+        min(i, rows-1)) replaces the single ``beta``."""
         llr = np.ascontiguousarray(llr, dtype=np.int8).reshape(-1, code.n)
         n = llr.shape[0]
         post = np.zeros_like(llr)
         it = np.zeros(n, np.uint32)
         cs, keep = self._code(code)
+        if beta_table is not None:
+            b = np.ascontiguousarray(beta_table, dtype=np.int8)
+            assert b.ndim == 2 and b.shape[1] == code.mrow
+            self.lib.orc_decode_int8_table(C.byref(cs), llr.ctypes.data_as(C.c_void_p), C.c_size_t(n),
+                                           C.c_uint(max_iter), C.c_float(max_row_metric), b.ctypes.data_as(C.c_void_p),
+                                           C.c_int(b.shape[0]), post.ctypes.data_as(C.c_void_p),
+                                           it.ctypes.data_as(C.c_void_p))
+            return post, it
         if beta_layers is not None:
             b = np.ascontiguousarray(beta_layers, dtype=np.int8)
             assert b.size == code.mrow

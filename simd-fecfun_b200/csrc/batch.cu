@@ -22,6 +22,8 @@ struct ldpc_batch {
     std::vector<ldpc_code> codes;
     std::vector<ldpc_cfg> cfgs;
     std::vector<std::vector<int>> beta8;     // per code, per layer
+    std::vector<std::vector<int>> tab8;      // per code: int8 offset table [rows][layer], or empty
+    std::vector<int> tab_rows;
     std::vector<uint32_t> maxv2;
     int tuned_threads = 0, tuned_cpc = 0;    // one launch shape for all codes (float, or one class)
     std::vector<int> code_threads, code_cpc;  // int8 per-class tuning, per code (0 = untuned)
@@ -39,6 +41,7 @@ struct ldpc_batch_plan {
     void* d_jobs = nullptr;
     ldpc::RtChunk* d_chunks = nullptr;
     void* d_scratch = nullptr;
+    uint16_t* d_tabs = nullptr;              // offset tables of the plan's codes (half bits)
     unsigned int* d_claim = nullptr;        // chunk-claim counter, zeroed before each launch
     cudaStream_t own = nullptr;              // graph capture and replay stream
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
@@ -126,6 +129,7 @@ void release(ldpc_batch_plan* p) {
     cudaFree(p->d_jobs);
     cudaFree(p->d_chunks);
     cudaFree(p->d_scratch);
+    cudaFree(p->d_tabs);
     cudaFree(p->d_claim);
 }
 
@@ -282,6 +286,7 @@ int int8_plan(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int threads
         dmax = std::max(dmax, ldpc::rt_dmax(cd.max_row_weight));
         maxE = std::max(maxE, E);
         for (int v : b->beta8[c]) quirk |= v == 0;
+        for (int v : b->tab8[c]) quirk |= v == 0;
     }
     size_t smem = 0;
     for (int c = 0; c < nc; ++c) {
@@ -305,6 +310,23 @@ int int8_plan(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int threads
         const ldpc_code& cd = b->codes[c];
         if (int rc = ldpc::make_rt_code(cd, (int)b->cfgs[c].max_iter, b->maxv2[c], b->beta8[c].data(), 0, G[c], &hc[c]))
             return rc;
+    }
+    // offset tables of the used codes, one device buffer
+    std::vector<uint16_t> tabs;
+    std::vector<size_t> tab_at(nc, 0);
+    for (int c = 0; c < nc; ++c) {
+        if (!used[c] || b->tab8[c].empty()) continue;
+        tab_at[c] = tabs.size();
+        for (int v : b->tab8[c]) tabs.push_back((uint16_t)ldpc::half2_bits((float)v));
+    }
+    if (!tabs.empty()) {
+        CUDA_TRY(cudaMalloc(&p->d_tabs, tabs.size() * sizeof(uint16_t)));
+        CUDA_TRY(cudaMemcpy(p->d_tabs, tabs.data(), tabs.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+        for (int c = 0; c < nc; ++c) {
+            if (!used[c] || b->tab8[c].empty()) continue;
+            hc[c].beta_tab = p->d_tabs + tab_at[c];
+            hc[c].tab_rows = b->tab_rows[c];
+        }
     }
     std::vector<ldpc::RtJob> hj(n_jobs);
     std::vector<long long> cost(n_jobs);
@@ -382,6 +404,7 @@ int int8_class(const ldpc_batch* b, int c, int threads, PlanClass* out) {
     const bool rsmem = ldpc::rt_smem_bytes(n, G, E, threads, true) <= (size_t)ldpc::kRtMaxSmem;
     bool quirk = false;
     for (int v : b->beta8[c]) quirk |= v == 0;
+    for (int v : b->tab8[c]) quirk |= v == 0;
     const int dmax = ldpc::rt_dmax(cd.max_row_weight);
     ldpc::rt_fn k = ldpc::rt_kernel_for(dmax, quirk, rsmem);
     CUDA_TRY(ldpc::allow_dynamic_smem((const void*)k, ldpc::kRtMaxSmem));
@@ -523,6 +546,8 @@ int ldpc_batch_create(const ldpc_code* const* codes, const ldpc_cfg* cfgs, int n
             b->codes.push_back(c);
             b->cfgs.push_back(g);
             b->beta8.push_back(std::vector<int>(c.mrow, 0));
+            b->tab8.emplace_back();
+            b->tab_rows.push_back(0);
             b->maxv2.push_back(0);
             b->maxf.push_back(g.max_row_metric < 1e-6f ? (float)(1.0 - (double)g.max_row_metric) : g.max_row_metric);
             continue;
@@ -540,6 +565,8 @@ int ldpc_batch_create(const ldpc_code* const* codes, const ldpc_cfg* cfgs, int n
         b->codes.push_back(c);
         b->cfgs.push_back(g);
         b->beta8.push_back(std::vector<int>(c.mrow, (int)(int8_t)g.beta));
+        b->tab8.emplace_back();
+        b->tab_rows.push_back(0);
         b->maxv2.push_back(ldpc::half2_bits((float)max8));
         b->maxf.push_back(0.f);
     }
@@ -557,6 +584,28 @@ int ldpc_batch_set_offsets(ldpc_batch* b, int code, const float* beta) {
         if (!(f >= 0.0f && f < 128.0f)) return fail(LDPC_ERR_UNSUPPORTED, "offset %g of layer %zu outside [0, 128)", f, l);
     }
     for (size_t l = 0; l < v.size(); ++l) v[l] = (int)(int8_t)(beta ? beta[l] : b->cfgs[code].beta);
+    b->tab8[code].clear();
+    b->tab_rows[code] = 0;
+    return LDPC_OK;
+}
+
+int ldpc_batch_set_offset_table(ldpc_batch* b, int code, const float* beta, unsigned rows) {
+    if (!b) return fail(LDPC_ERR_INVALID_ARG, "batch is NULL");
+    if (b->variant != LDPC_INT8_OMS) return fail(LDPC_ERR_UNSUPPORTED, "offset tables are for int8 batches");
+    if (code < 0 || code >= (int)b->codes.size()) return fail(LDPC_ERR_INVALID_ARG, "code %d of %zu", code, b->codes.size());
+    if (beta && (rows < 1 || rows > 255)) return fail(LDPC_ERR_INVALID_ARG, "offset table of %u rows (1..255)", rows);
+    const size_t m = (size_t)b->codes[code].mrow;
+    std::vector<int> tab;
+    if (beta) {
+        for (size_t i = 0; i < rows * m; ++i) {
+            if (!(beta[i] >= 0.0f && beta[i] < 128.0f))
+                return fail(LDPC_ERR_UNSUPPORTED, "offset %g of row %zu, layer %zu outside [0, 128)", beta[i], i / m, i % m);
+            tab.push_back((int)(int8_t)beta[i]);
+        }
+    }
+    b->tab8[code] = tab;
+    b->tab_rows[code] = beta ? (int)rows : 0;
+    std::fill(b->beta8[code].begin(), b->beta8[code].end(), (int)(int8_t)b->cfgs[code].beta);
     return LDPC_OK;
 }
 

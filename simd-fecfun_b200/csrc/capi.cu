@@ -326,6 +326,31 @@ int ldpc_ctx_create(const ldpc_code* code, const ldpc_cfg* cfg, int device, ldpc
     return LDPC_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// Rebuild an int8 context's decoder with new offsets (per layer, or a
+// [rows][layer] table; both empty = cfg.beta).
+int reset_offsets(ldpc_ctx* x, const std::vector<int>& layers, const std::vector<int>& tab, int rows) {
+    CUDA_TRY(cudaSetDevice(x->device));
+    CUDA_TRY(cudaDeviceSynchronize());   // no launch of this context may still use the old descriptor
+    cudaFree(x->d_rt_code);
+    cudaFree(x->d_rt_scratch);
+    cudaFree(x->d_beta_tab);
+    x->d_rt_code = nullptr;
+    x->d_rt_scratch = nullptr;
+    x->d_beta_tab = nullptr;
+    x->oms_rt = false;
+    x->inst = nullptr;
+    x->layer_beta8 = layers;
+    x->tab_beta8 = tab;
+    x->tab_rows = rows;
+    return ldpc::setup_oms(x);
+}
+}  // namespace
+
+extern "C" {
+
 int ldpc_ctx_set_layer_offsets(ldpc_ctx* x, const float* beta) {
     if (!x) return fail(LDPC_ERR_INVALID_ARG, "ctx is NULL");
     if (x->cfg.variant != LDPC_INT8_OMS) return fail(LDPC_ERR_UNSUPPORTED, "per-layer offsets are for int8 contexts");
@@ -337,16 +362,23 @@ int ldpc_ctx_set_layer_offsets(ldpc_ctx* x, const float* beta) {
             table.push_back((int)(int8_t)beta[l]);   // truncated like cfg.beta (decode_functions.cpp:60)
         }
     }
-    CUDA_TRY(cudaSetDevice(x->device));
-    CUDA_TRY(cudaDeviceSynchronize());   // no launch of this context may still use the old descriptor
-    cudaFree(x->d_rt_code);
-    cudaFree(x->d_rt_scratch);
-    x->d_rt_code = nullptr;
-    x->d_rt_scratch = nullptr;
-    x->oms_rt = false;
-    x->inst = nullptr;
-    x->layer_beta8 = table;
-    return ldpc::setup_oms(x);
+    return reset_offsets(x, table, {}, 0);
+}
+
+int ldpc_ctx_set_offset_table(ldpc_ctx* x, const float* beta, unsigned rows) {
+    if (!x) return fail(LDPC_ERR_INVALID_ARG, "ctx is NULL");
+    if (x->cfg.variant != LDPC_INT8_OMS) return fail(LDPC_ERR_UNSUPPORTED, "offset tables are for int8 contexts");
+    if (beta && (rows < 1 || rows > 255)) return fail(LDPC_ERR_INVALID_ARG, "offset table of %u rows (1..255)", rows);
+    std::vector<int> tab;
+    if (beta) {
+        const size_t m = (size_t)x->code.mrow;
+        for (size_t i = 0; i < rows * m; ++i) {
+            if (!(beta[i] >= 0.0f && beta[i] < 128.0f))
+                return fail(LDPC_ERR_UNSUPPORTED, "offset %g of row %zu, layer %zu outside [0, 128)", beta[i], i / m, i % m);
+            tab.push_back((int)(int8_t)beta[i]);   // truncated like cfg.beta (decode_functions.cpp:60)
+        }
+    }
+    return reset_offsets(x, {}, tab, beta ? (int)rows : 0);
 }
 
 void ldpc_ctx_destroy(ldpc_ctx* x) {
@@ -359,6 +391,7 @@ void ldpc_ctx_destroy(ldpc_ctx* x) {
     cudaFree(x->d_int_scratch);
     cudaFree(x->d_rt_code);
     cudaFree(x->d_rt_scratch);
+    cudaFree(x->d_beta_tab);
     for (int i = 0; i < 2; ++i) {
         if (x->streams[i]) cudaStreamDestroy(x->streams[i]);
         for (int k = 0; k < 4; ++k) cudaFree(x->d_pipe[i][k]);

@@ -79,8 +79,9 @@ int setup_oms(ldpc_ctx* x) {
     const ldpc_code& c = x->code;
     const int L = c.mrow;
     // LDPC_OMS_RT forces the run-time-table kernel (tuning and cross-checks);
-    // per-layer offsets need it too (the compiled shapes take one offset)
-    if (getenv("LDPC_OMS_RT") || !x->layer_beta8.empty()) return setup_oms_rt(x);
+    // per-layer offsets and offset tables need it too (the compiled shapes
+    // take one offset)
+    if (getenv("LDPC_OMS_RT") || !x->layer_beta8.empty() || x->tab_rows) return setup_oms_rt(x);
     const OmsInst* best = nullptr;
     const bool use_compiled = !getenv("LDPC_OMS_NO_COMPILED");
     const bool use_split = !getenv("LDPC_OMS_NO_SPLIT");

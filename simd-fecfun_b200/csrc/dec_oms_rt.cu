@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
 #include "internal.h"
 #include "oms_rt.cuh"
@@ -99,8 +100,17 @@ int setup_oms_rt(ldpc_ctx* x) {
     const int* table = x->layer_beta8.empty() ? nullptr : x->layer_beta8.data();
     int rc = make_rt_code(c, (int)x->cfg.max_iter, x->maxv2, table, (int)(int8_t)x->cfg.beta, G, &host);
     if (rc) return rc;
-    bool quirk = x->layer_beta8.empty() && x->beta0;
+    bool quirk = x->layer_beta8.empty() && !x->tab_rows && x->beta0;
     for (int v : x->layer_beta8) quirk |= v == 0;
+    for (int v : x->tab_beta8) quirk |= v == 0;
+    if (x->tab_rows) {
+        std::vector<uint16_t> h(x->tab_beta8.size());
+        for (size_t i = 0; i < h.size(); ++i) h[i] = (uint16_t)half2_bits((float)x->tab_beta8[i]);
+        CUDA_TRY(cudaMalloc(&x->d_beta_tab, h.size() * sizeof(uint16_t)));
+        CUDA_TRY(cudaMemcpy(x->d_beta_tab, h.data(), h.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+        host.beta_tab = x->d_beta_tab;
+        host.tab_rows = x->tab_rows;
+    }
     rt_fn k = rt_kernel_for(dmax, quirk, rsmem);
     CUDA_TRY(allow_dynamic_smem((const void*)k, kRtMaxSmem));
     int per_sm = 0;

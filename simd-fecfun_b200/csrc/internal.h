@@ -97,6 +97,9 @@ struct ldpc_ctx {
     uint32_t beta2 = 0, maxv2 = 0;
     bool beta0 = false;
     std::vector<int> layer_beta8;               // per-layer int8 offsets (ldpc_ctx_set_layer_offsets), empty = cfg.beta
+    std::vector<int> tab_beta8;                 // int8 offset table [tab_rows][mrow] (ldpc_ctx_set_offset_table)
+    int tab_rows = 0;
+    uint16_t* d_beta_tab = nullptr;             // the table as half bits, on the device
     int oms_synd_loop = 0;                      // syndrome as a table loop (tuning: LDPC_OMS_SYND_LOOP)
     // int8 offset min-sum over run-time tables (shapes without a compiled kernel)
     bool oms_rt = false;

@@ -19,13 +19,27 @@
 
 namespace ldpc {
 
+// Offset (half2 bits) and beta = 0 quirk mask of layer l for the two
+// codewords of a pair, at iterations it0 (low lane) and it1 (high lane).
+__device__ __forceinline__ void rt_offsets(const RtCode& C, int l, int it0, int it1, uint32_t& beta2, uint32_t& quirk) {
+    if (!C.beta_tab) {
+        beta2 = C.beta2[l];
+        quirk = C.quirk2[l];
+        return;
+    }
+    const int last = C.tab_rows - 1;
+    const uint32_t b0 = C.beta_tab[(it0 < last ? it0 : last) * C.L + l];
+    const uint32_t b1 = C.beta_tab[(it1 < last ? it1 : last) * C.L + l];
+    beta2 = b0 | (b1 << 16);
+    quirk = (b0 ? 0u : 0x0000d800u) | (b1 ? 0u : 0xd8000000u);
+}
+
 template <int DMAX, bool QUIRK>
 __device__ __forceinline__ void rt_layer(const RtCode& C, int l, uint32_t* Ps, uint32_t* Rt, int nthr, int t, int gbase,
-                                         int z) {
+                                         int z, uint32_t beta2, uint32_t quirk_l) {
     constexpr uint32_t SGN = 0x80008000u;
     const int d = C.rw[l], eb = C.ebase[l];
-    const uint32_t beta2 = C.beta2[l];
-    const uint32_t quirk = QUIRK ? C.quirk2[l] : 0u;
+    const uint32_t quirk = QUIRK ? quirk_l : 0u;
     uint32_t q[DMAX];
     int addr[DMAX];
     uint32_t mn1 = H2_1024, mn2 = H2_1024;
@@ -217,9 +231,16 @@ __global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtL
 
         for (int par = 0;; par ^= 1) {
             // ---------------- one layered iteration ----------------
+            // iteration index of this thread's two codewords (offset tables)
+            const int it0 = s_it[2 * g], it1 = s_it[2 * g + 1];
             for (int l = 0; l < C.L; ++l) {
-                if (active)
-                    rt_dispatch<DMAX>(C.rw[l], [&](auto D) { rt_layer<decltype(D)::value, QUIRK>(C, l, Ps, Rt, nthr, t, gbase, z); });
+                if (active) {
+                    uint32_t beta2, quirk;
+                    rt_offsets(C, l, it0, it1, beta2, quirk);
+                    rt_dispatch<DMAX>(C.rw[l], [&](auto D) {
+                        rt_layer<decltype(D)::value, QUIRK>(C, l, Ps, Rt, nthr, t, gbase, z, beta2, quirk);
+                    });
+                }
                 __syncthreads();
             }
             if (tid < 16) {

@@ -90,6 +90,8 @@ struct alignas(16) RtCode {
     uint32_t maxv2;                  // half2 bits of Max8
     uint32_t beta2[RT_MAX_L];        // half2 bits of beta8 per layer
     uint32_t quirk2[RT_MAX_L];       // -128.0 in both lanes where beta8 = 0 (abs8(-128) = -128), else 0
+    const uint16_t* beta_tab;        // or null: half bits of beta8 per [row][layer]; a codeword's iteration i
+    int tab_rows;                    //   (0-based) uses row min(i, tab_rows - 1), in place of beta2 / quirk2
     int16_t rw[RT_MAX_L];
     int16_t ebase[RT_MAX_L];         // first edge of layer l
     uint32_t edge[RT_MAX_E];         // (column * Z) << 9 | shift

@@ -77,6 +77,8 @@ _PROTOS = {
     "ldpc_ctx_create": (C.c_int, [_vp, C.POINTER(Cfg), C.c_int, C.POINTER(_vp)]),
     "ldpc_ctx_destroy": (None, [_vp]),
     "ldpc_ctx_set_layer_offsets": (C.c_int, [_vp, _vp]),
+    "ldpc_ctx_set_offset_table": (C.c_int, [_vp, _vp, C.c_uint]),
+    "ldpc_batch_set_offset_table": (C.c_int, [_vp, C.c_int, _vp, C.c_uint]),
     "ldpc_decode_int8": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _vp]),
     "ldpc_decode_f32": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _vp]),
     "ldpc_decode_int16": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _vp]),
@@ -228,6 +230,15 @@ class Context:
         b = np.ascontiguousarray(beta_per_layer, dtype=np.float32)
         check(lib.ldpc_ctx_set_layer_offsets(self.h, b.ctypes.data))
 
+    def set_offset_table(self, beta=None):
+        """int8 contexts: offsets beta[rows][layers]; iteration i uses row
+        min(i, rows-1) (None restores cfg.beta)."""
+        if beta is None:
+            check(lib.ldpc_ctx_set_offset_table(self.h, None, 0))
+            return
+        b = np.ascontiguousarray(beta, dtype=np.float32)
+        check(lib.ldpc_ctx_set_offset_table(self.h, b.ctypes.data, b.shape[0]))
+
     # ---- device-pointer API (torch tensors) ----
     def decode_int8(self, llr, n, post=None, hard=None, iters=None, stream=0):
         check(lib.ldpc_decode_int8(self.h, _ptr(llr), n, _ptr(post), _ptr(hard), _ptr(iters), stream or None))
@@ -339,6 +350,15 @@ class Batch:
             return
         b = np.ascontiguousarray(beta_per_layer, dtype=np.float32)
         check(lib.ldpc_batch_set_offsets(self.h, code, b.ctypes.data))
+
+    def set_offset_table(self, code: int, beta=None):
+        """int8 batches: offsets beta[rows][layers] for one code; iteration i
+        uses row min(i, rows-1) (None restores cfg.beta)."""
+        if beta is None:
+            check(lib.ldpc_batch_set_offset_table(self.h, code, None, 0))
+            return
+        b = np.ascontiguousarray(beta, dtype=np.float32)
+        check(lib.ldpc_batch_set_offset_table(self.h, code, b.ctypes.data, b.shape[0]))
 
     @staticmethod
     def _jobs(specs):

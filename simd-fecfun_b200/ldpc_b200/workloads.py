@@ -8,8 +8,8 @@
   The same jobs decoded one code at a time are timed beside it.
 * :func:`hetero_mix` -- every 802.11n code, 802.11ay 1/2..7/8 and 802.11ad
   13/16 in one launch, each at the SNR calibrated to codeword error rate
-  near 1e-3: plain offsets vs learned per-layer offsets (trained in float,
-  quantised to int8).
+  near 1e-3: plain offsets vs learned per-(iteration, layer) offsets
+  (trained in float, quantised to an int8 table).
 * :func:`learned_run` -- training throughput of the learned-offset decoder
   (802.16e 1/2, Z=96, 10 iterations x 12 layers, batches of 65536
   codewords), then codeword error rate and average iterations of learned
@@ -193,8 +193,9 @@ def hetero_mix(steps: int = 3, warmup: int = 1, total: int = 10_000_000, seed: i
     plan = batch.plan(specs)
     ms_plain = _time_plan(plan, specs, steps, warmup)
     q_plain = _quality(specs, meta, names, objs, steps)
-    # learned per-layer offsets: float offset min-sum trained at the code's SNR,
-    # averaged over iterations, converted to int8 LLR units (scale 2) and rounded
+    # learned offsets: float offset min-sum trained at the code's SNR,
+    # converted to int8 LLR units (scale 2), rounded, and decoded as an int8
+    # [iteration][layer] table
     t0 = time.time()
     offsets = []
     for ci, (h, c) in enumerate(zip(handles, objs)):
@@ -203,8 +204,8 @@ def hetero_mix(steps: int = 3, warmup: int = 1, total: int = 10_000_000, seed: i
         eb = snr[ci] - 10.0 * math.log10(_rate(c))
         beta, _ = learned.train(fctx, c, iters=10, batch=8192, steps=train_steps, ebn0=(eb - 0.25, eb + 0.25), lr=0.02,
                                 init=0.5, seed=seed + ci, n_snr=4)
-        b8 = np.clip(np.rint(2.0 * beta.mean(dim=0).cpu().numpy()), 0, 127).astype(np.float32)
-        batch.set_offsets(ci, b8)
+        b8 = np.clip(np.rint(2.0 * beta.cpu().numpy()), 0, 127).astype(np.float32)   # [iters][layers]
+        batch.set_offset_table(ci, b8)
         offsets.append(b8.astype(int).tolist())
     train_s = time.time() - t0
     plan_l = batch.plan(specs)
@@ -228,8 +229,8 @@ def hetero_mix(steps: int = 3, warmup: int = 1, total: int = 10_000_000, seed: i
         "learned": {"value": total / (avg_learned * 1e-3), "unit": "codewords/s", "avg_iter": it_l,
                     "offsets_int8": dict(zip(names, offsets)), "training_s": round(train_s, 1),
                     "training": "float offset min-sum, 10 iterations, %d Adam steps of 8192 codewords at the "
-                                "calibrated SNR +-0.25 dB; offsets averaged over iterations, x2 (int8 LLR scale), "
-                                "rounded" % train_steps},
+                                "calibrated SNR +-0.25 dB; offsets x2 (int8 LLR scale), rounded, deployed as an "
+                                "int8 [iteration][layer] table" % train_steps},
         "plain_avg_iter": it_p,
         "gpu_launches": steps * plan.kernels,
         "quality_plain": q_plain, "quality_learned": q_learned,

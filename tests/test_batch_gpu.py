@@ -45,7 +45,9 @@ def _mix(capi, oracle):
 def _verify(oracle, objs, handles, data, bufs, betas=None):
     for i, (name, kw, snr, n, it, beta) in enumerate(MIX):
         llr, _ = data[i]
-        if betas is not None and betas[i] is not None:
+        if betas is not None and betas[i] is not None and betas[i].ndim == 2:
+            post_o, it_o = oracle.decode_int8(objs[i], llr, it, 31.0, beta_table=betas[i])
+        elif betas is not None and betas[i] is not None:
             post_o, it_o = oracle.decode_int8(objs[i], llr, it, 31.0, beta_layers=betas[i])
         else:
             post_o, it_o = oracle.decode_int8(objs[i], llr, it, 31.0, beta)
@@ -106,6 +108,33 @@ def test_per_layer_offsets(capi, oracle):
     plan = batch.plan(specs)
     _clear(bufs)
     plan.launch()
+    torch.cuda.synchronize()
+    _verify(oracle, objs, handles, data, bufs, betas)
+
+
+def test_offset_tables(capi, oracle):
+    """Learned per-(iteration, layer) offsets quantised to int8: a table for
+    some codes (rows = max_iter, or fewer: the last row repeats), per-layer
+    offsets for one, plain beta for the rest; the two codewords of a pair
+    run at different iterations, each with its own row."""
+    import torch
+    batch, objs, handles, data, specs, bufs = _mix(capi, oracle)
+    rng = np.random.default_rng(12)
+    betas = [None] * len(objs)
+    for i, c in enumerate(objs):
+        rows = MIX[i][4] if i % 3 == 0 else 4
+        if i % 3 == 2:
+            b = rng.integers(0, 4, c.mrow).astype(np.float32) + np.float32(0.5)
+            batch.set_offsets(i, b)
+            betas[i] = b.astype(np.int8)
+        else:
+            t = rng.integers(0, 4, (rows, c.mrow)).astype(np.float32) + np.float32(0.5)
+            t[rows - 1, 0] = 0.0
+            batch.set_offset_table(i, t)
+            betas[i] = t.astype(np.int8)
+    plan = batch.plan(specs)
+    _clear(bufs)
+    plan.graph_launch(torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
     _verify(oracle, objs, handles, data, bufs, betas)
 

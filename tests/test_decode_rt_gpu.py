@@ -209,3 +209,34 @@ def test_context_layer_offsets(capi, oracle, name, snr):
     assert np.array_equal(post, post_o) and np.array_equal(iters, it_o.astype(np.uint8))
     with pytest.raises(capi.LdpcError):
         ctx.set_layer_offsets(np.full(code.mrow, 300.0, np.float32))
+
+
+@pytest.mark.parametrize("name,snr,rows", [("11ad 1/2", -0.5, 12), ("11ad 1/2", -0.5, 3), ("5GNR_n1000_k500", -1.0, 20)])
+def test_context_offset_table(capi, oracle, name, snr, rows):
+    """ldpc_ctx_set_offset_table: iteration i uses row min(i, rows-1) (rows
+    shorter than max_iter included), offsets 0..3 with zeros (the abs8(-128)
+    quirk); then the per-layer form replaces it, and None restores beta."""
+    from ldpc_b200 import codes
+    code = codes.code_by_name(name)
+    max_iter = 12 if rows != 20 else 20
+    llr, _, _ = make_llr_int8(code, 500, snr, seed=41, oracle=oracle)
+    ctx = capi.Context(capi.Code.from_tables(code), max_iter=max_iter, beta=1.0)
+    rng = np.random.default_rng(rows)
+    tab = rng.integers(0, 4, (rows, code.mrow)).astype(np.float32) + np.float32(0.25)
+    tab[0, 0] = 0.0
+    ctx.set_offset_table(tab)
+    post, hard, iters, tot = ctx.decode_host(llr)
+    post_o, it_o = oracle.decode_int8(code, llr, max_iter, 31.0, beta_table=tab.astype(np.int8))
+    assert np.array_equal(iters, it_o.astype(np.uint8)) and np.array_equal(post, post_o)
+    kb = ctx.info.kbits
+    assert np.array_equal(hard, pack_bits((post_o[:, :kb] < 0).astype(np.uint8)))
+    ctx.set_layer_offsets(tab[1])
+    post, hard, iters, tot = ctx.decode_host(llr)
+    post_o, it_o = oracle.decode_int8(code, llr, max_iter, 31.0, beta_layers=tab[1].astype(np.int8))
+    assert np.array_equal(iters, it_o.astype(np.uint8)) and np.array_equal(post, post_o)
+    ctx.set_offset_table(None)
+    post, hard, iters, tot = ctx.decode_host(llr)
+    post_o, it_o = oracle.decode_int8(code, llr, max_iter, 31.0, 1.0)
+    assert np.array_equal(iters, it_o.astype(np.uint8)) and np.array_equal(post, post_o)
+    with pytest.raises(capi.LdpcError):
+        ctx.set_offset_table(np.full((2, code.mrow), 128.0, np.float32))
