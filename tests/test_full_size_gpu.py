@@ -54,6 +54,34 @@ def test_noiseless_round_trip_full_size(capi):
     assert int(llr.abs().min()) == 24     # every LLR at the clip: no noise got through
 
 
+@pytest.mark.parametrize("name,variant,n", [("5GNR_n25344_k8448", "LDPC_INT8_OMS", 200_000),
+                                            ("5GNR_n3136_k576", "LDPC_INT8_OMS", 1_000_000),
+                                            ("16e 1/2", "LDPC_F32_SP", 1_000_000)])
+def test_noiseless_round_trip_other_codes(capi, name, variant, n):
+    """Punctured columns (LLR 0) and filler bits (LLR +max) of 5G NR, and the
+    float sum-product decoder: zero errors on every codeword."""
+    import torch
+    from ldpc_b200 import codes
+    code = codes.code_by_name(name) if name.startswith("5G") else codes.make_code(name, z_over=96)
+    v = getattr(capi, variant)
+    fl = v != capi.LDPC_INT8_OMS
+    ctx = capi.Context(capi.Code.from_tables(code), variant=v, max_iter=20, max_row_metric=6e-8 if fl else 31.0,
+                       beta=0.0 if fl else 1.0, llr_scale=1.0 if fl else 2.0, max_abs_llr=1e9 if fl else 24.0)
+    llr = torch.empty((1, n, code.n), dtype=torch.float32 if fl else torch.int8, device="cuda")
+    data = torch.empty((n, ctx.info.hard_words), dtype=torch.int32, device="cuda")
+    if fl:
+        ctx.generate(seed=11, cw_offset=0, snr_db=[40.0], n_per_snr=n, llr_f32=llr, data_bits=data)
+    else:
+        ctx.generate(seed=11, cw_offset=0, snr_db=[40.0], n_per_snr=n, llr_int=llr, data_bits=data)
+    cnt = torch.zeros((1, 4), dtype=torch.int64, device="cuda")
+    iters = torch.empty(n, dtype=torch.uint8, device="cuda")
+    ctx.decode_count(llr[0], n, iters=iters, data_bits=data, ref_period=n, bucket_size=n, counters=cnt, n_buckets=1)
+    torch.cuda.synchronize()
+    c = cnt.cpu().numpy()[0].tolist()
+    assert c[0] == n and c[2] == 0 and c[3] == 0
+    assert int(iters.max()) < 20 and c[1] == int(iters.sum())
+
+
 def test_launch_split_and_early_exit_full_size(capi):
     import torch
     from ldpc_b200 import codes
