@@ -334,18 +334,30 @@ namespace {
 int reset_offsets(ldpc_ctx* x, const std::vector<int>& layers, const std::vector<int>& tab, int rows) {
     CUDA_TRY(cudaSetDevice(x->device));
     CUDA_TRY(cudaDeviceSynchronize());   // no launch of this context may still use the old descriptor
-    cudaFree(x->d_rt_code);
-    cudaFree(x->d_rt_scratch);
-    cudaFree(x->d_beta_tab);
-    x->d_rt_code = nullptr;
-    x->d_rt_scratch = nullptr;
-    x->d_beta_tab = nullptr;
-    x->oms_rt = false;
-    x->inst = nullptr;
-    x->layer_beta8 = layers;
-    x->tab_beta8 = tab;
-    x->tab_rows = rows;
-    return ldpc::setup_oms(x);
+    auto rebuild = [x](const std::vector<int>& ly, const std::vector<int>& tb, int r) {
+        cudaFree(x->d_rt_code);
+        cudaFree(x->d_rt_scratch);
+        cudaFree(x->d_beta_tab);
+        x->d_rt_code = nullptr;
+        x->d_rt_scratch = nullptr;
+        x->d_beta_tab = nullptr;
+        x->oms_rt = false;
+        x->inst = nullptr;
+        x->layer_beta8 = ly;
+        x->tab_beta8 = tb;
+        x->tab_rows = r;
+        return ldpc::setup_oms(x);
+    };
+    const std::vector<int> old_layers = x->layer_beta8, old_tab = x->tab_beta8;
+    const int old_rows = x->tab_rows;
+    const int rc = rebuild(layers, tab, rows);
+    if (rc != LDPC_OK) {
+        // keep the context usable with its previous offsets; report the failure
+        const std::string why = ldpc_last_error();
+        rebuild(old_layers, old_tab, old_rows);
+        return fail(rc, "%s", why.c_str());
+    }
+    return LDPC_OK;
 }
 }  // namespace
 
