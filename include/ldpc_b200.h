@@ -193,21 +193,22 @@ int ldpc_decode_int32_host(ldpc_ctx *ctx, const int32_t *llr, size_t n, int32_t 
 int ldpc_decode_set_compat(ldpc_ctx *ctx, void *decoded_metrics, unsigned num_codeword, unsigned simd_par,
                            uint64_t *tot_iter);
 
-/* ---- batched decoding of several codes in one launch ----------------------
+/* ---- batched decoding of several codes in one graph ------------------------
  *
  * No counterpart in the reference: it runs one code per process
  * (build/run_LDPCsim.pl:102-109) and one codeword at a time
  * (LDPCdecode.cpp:227-243).  A batch holds several codes, each with its own
  * configuration; all codes use the same variant (LDPC_INT8_OMS, LDPC_F32_SP or
- * LDPC_F32_OMS).  int8 batches also take one int8 offset per layer (learned
- * offsets).  A plan fixes a list of jobs (device buffers
- * of one code each) and splits them into chunks of equal work.  A plan's
- * launch is one persistent kernel over all jobs -- for int8 plans, one per
- * geometry class: jobs whose codes would run at different occupancies get
- * separate launches -- and it can be replayed from a CUDA graph (one kernel
- * node per class, free to overlap).  CTAs claim chunks from a per-launch
- * counter, so a plan's launches on different streams must not overlap.  Per codeword, the results are exactly
- * those of ldpc_decode_int8 / ldpc_decode_count on that code. */
+ * LDPC_F32_OMS).  int8 batches also take offsets per layer or per
+ * (iteration, layer) (learned offsets).  A plan fixes a list of jobs (device
+ * buffers of one code each) and splits them into chunks of equal work.  A
+ * plan's launch is one persistent kernel per geometry class (codes that
+ * would run at the same occupancy share one; LDPC_BATCH_ONE_LAUNCH forces a
+ * single kernel), and it can be replayed from a CUDA graph with one kernel
+ * node per class, free to overlap.  CTAs claim chunks from a per-launch
+ * counter, so launches of one plan on different streams must not overlap.
+ * Per codeword, the results are exactly those of ldpc_decode_int8 /
+ * ldpc_decode_count on that code. */
 typedef struct ldpc_batch ldpc_batch;
 typedef struct ldpc_batch_plan ldpc_batch_plan;
 
