@@ -85,8 +85,8 @@ def test_matches_live_reference_build(capi, oracle, mode):
     if not rb.ref_available(variant):
         pytest.skip("reference build %s absent" % variant)
     lib = rb.RefLib(variant)
-    for name, snr in (("11n 2/3 z54", 2.5), ("11ay 5/8", 1.0), ("16e 3/4A", 2.0)):
-        code = codes.make_code(name, elem_size=64)
+    for name, snr in (("11n 2/3 z54", 2.5), ("11ay 5/8", 1.0), ("16e 3/4A", 2.0), ("5GNR_n1000_k500", -1.0)):
+        code = codes.code_by_name(name, elem_size=64)
         llr, _ = _llr(oracle, code, 24, snr, 4)
         ref = rb.RefCtx(lib, code, 24)
         ref.set_llr(llr)

@@ -46,10 +46,11 @@ def _check(capi, code, llr, bits, max_iter=10, mrm=31.0, beta=1.0):
 
 
 @pytest.mark.parametrize("bits", [16, 32])
-@pytest.mark.parametrize("name", ["11ad 1/2", "16e 1/2", "11n 5/6 z81", "ITU G.hn 1/2 z14"])
+@pytest.mark.parametrize("name", ["11ad 1/2", "16e 1/2", "11n 5/6 z81", "ITU G.hn 1/2 z14", "5GNR_n1000_k500",
+                                  "5GNR_n3136_k576"])
 def test_matches_reference_decoder(capi, oracle, bits, name):
     from ldpc_b200 import codes
-    code = codes.make_code(name, elem_size=bits)     # the reference build's SIMD layout
+    code = codes.code_by_name(name, elem_size=bits)  # the reference build's SIMD layout
     llr = _llr(code, 150, bits, 40.0, 1000, 3, oracle)
     _check(capi, code, llr, bits, mrm=400.0, beta=7.0)
 
