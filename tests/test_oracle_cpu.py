@@ -75,8 +75,8 @@ def test_oracle_matches_live_reference_build(oracle):
         pytest.skip("reference build oracle/_ref absent")
     lib = rb.RefLib("Vec64c_min")
     rng = np.random.default_rng(0)
-    for name in ("11ad 13/16", "16e 5/6", "11n 2/3 z54", "11ay 1/2", "ITU G.hn 1/2 z14"):
-        code = codes.make_code(name)
+    for name in ("11ad 13/16", "16e 5/6", "11n 2/3 z54", "11ay 1/2", "ITU G.hn 1/2 z14", "5GNR_n1000_k500"):
+        code = codes.code_by_name(name)
         ctx = rb.RefCtx(lib, code, 24)
         llr = rng.integers(-30, 31, (24, code.n)).astype(np.int8) + \
             np.where(rng.random((24, code.n)) < 0.5, 8, -8).astype(np.int8)
