@@ -292,6 +292,77 @@ def run_variants(args, clk):
     }
 
 
+def run_sim(args):
+    """--workload sim: the process-level drop-in against the reference's own
+    simulator.  ldpc_sim (linked as LDPCtop_Vec64c_min_b200) and the
+    reference's LDPCtop_Vec64c_min (built from its sources in oracle/_ref) get
+    the same stdin blob parameters (802.11ad 1/2, the Perl driver's defaults,
+    SNR -1.00..0.00 dB step 0.25, given seeds); the reference runs one process
+    per host core, as its Perl driver does.  Wall-clock time from process
+    start to exit covers everything a simulation does: noise and data
+    generation, encoding, decoding, error counting and start-up."""
+    import tempfile
+    from ldpc_b200 import codes, simproto
+    code = codes.make_code(CODE)
+    seeds = [(0x2545F4914F6CDD1D * (i + 1)) & ((1 << 56) - 1) for i in range(64)]
+    n_snr = len(SNRS)
+    sim = os.path.join(ROOT, "simd-fecfun_b200", "ldpc_b200", "ldpc_sim")
+    ref_exe = os.path.join(ROOT, "oracle", "_ref", "LDPCtop_Vec64c_min")
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        code.write_dat(os.path.join(d, "e.dat"), os.path.join(d, "d.dat"))
+        exe = os.path.join(d, "LDPCtop_Vec64c_min_b200")
+        os.symlink(sim, exe)
+
+        def run(path, per_snr, inner, procs=1):
+            data = simproto.blob(1, inner, per_snr // inner, MAX_ITER, MRM, SCALE, MAX_ABS, BETA, SNRS[0], SNRS[-1],
+                                 0.25, seeds, "e.dat", "d.dat")
+            t0 = time.perf_counter()
+            ps = [subprocess.Popen([path], stdin=subprocess.PIPE, stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                                   cwd=d) for _ in range(procs)]
+            for p in ps:   # every process gets its blob at once (820 bytes fit the pipe), then all run together
+                p.stdin.write(data)
+                p.stdin.close()
+            outs = [(p.stdout.read(), p.stderr.read()) for p in ps]
+            for p in ps:
+                p.wait(timeout=900)
+            wall = time.perf_counter() - t0
+            loops = []
+            for p, (o, e) in zip(ps, outs):
+                if p.returncode != 0:
+                    raise RuntimeError("%s exited %d: %s" % (path, p.returncode, (o + e).decode()[-500:]))
+                loops += simproto.parse(o.decode())["loops"]
+            cw = procs * (per_snr // inner) * inner * n_snr
+            cwe = sum(v[4] for v in loops)
+            return {"codewords": cw, "wall_s": wall, "value": cw / wall, "unit": "codewords/s",
+                    "cw_errors": cwe, "iterations": sum(v[2] for v in loops)}
+
+        run(exe, 10_000, 10)                       # warm: first-touch of the binary and the CUDA cache
+        out["gpu_startup"] = run(exe, 10, 1)        # one tiny run: the fixed cost (process, CUDA, tables), for context
+        gpu = run(exe, args.sim_n, 10)
+        ref = None
+        if os.path.exists(ref_exe):
+            threads = os.cpu_count() or 1
+            ref = run(ref_exe, args.sim_ref_n, 10, procs=threads)
+            ref.update({"cores": threads, "kind": "reference", "sample": "%d processes x %d codewords per SNR"
+                        % (threads, args.sim_ref_n)})
+    return {
+        "metric": "codewords/s simulated by the process-level drop-in (stdin blob to result lines), "
+                  "802.11ad rate-1/2, int8 offset min-sum, 10 max iterations",
+        "value": gpu["value"], "unit": "codewords/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
+        "data": "synthetic: each program's own generator (Philox on the GPU; the reference's sfc64/xoshiro and "
+                "normdist2 on the host)",
+        "config": {"workload": "802.11ad 1/2, SNR -1.00..0.00 dB step 0.25, %d codewords per SNR (GPU), beta=1, "
+                               "max_row_metric=31, LLR scale 2, max|LLR| 24, 10 max iterations" % args.sim_n,
+                   "timing": "wall clock from process start to exit, start-up included"},
+        "ldpc_sim": gpu, "gpu_startup": out["gpu_startup"],
+        "cpu_baseline": ref,
+        "speedup_vs_reference_processes": gpu["value"] / ref["value"] if ref else None,
+        "gpu_launches": None,
+    }
+
+
 def run_workload(args):
     """The other measured workloads (ldpc_b200.workloads), on one GPU; under
     torchrun only rank 0 runs."""
@@ -312,6 +383,8 @@ def run_workload(args):
                                  autotune=not args.no_autotune)
     elif args.workload == "variants":
         out = run_variants(args, clk)
+    elif args.workload == "sim":
+        out = run_sim(args)
     else:
         out = workloads.learned_run(train_steps=max(args.steps, 2), batch=args.learned_batch,
                                     weights=args.learned_weights)
@@ -333,13 +406,17 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--variant-n", type=int, default=200_000, help="codewords per SNR per variant (--workload variants)")
+    ap.add_argument("--sim-n", type=int, default=100_000_000, help="codewords per SNR for ldpc_sim (--workload sim)")
+    ap.add_argument("--sim-ref-n", type=int, default=100_000,
+                    help="codewords per SNR per reference process (--workload sim)")
     ap.add_argument("--variant-ref-sample", type=int, default=4000,
                     help="int8 codewords per host thread for the reference builds (--workload variants)")
     ap.add_argument("--workload", default="11ad",
-                    choices=["11ad", "nr-mix", "hetero-mix", "learned", "sp-sweep", "variants"],
+                    choices=["11ad", "nr-mix", "hetero-mix", "learned", "sp-sweep", "variants", "sim"],
                     help="11ad: the headline run; others: the batched 5G NR mix, the 18-code 802.11 mix "
                          "(plain vs learned offsets), learned-offset training, the float sum-product Z sweep, "
-                         "every decoder variant on the headline point (one GPU)")
+                         "every decoder variant on the headline point, the process-level drop-in against the "
+                         "reference's own simulator (one GPU)")
     ap.add_argument("--llr-budget-gb", type=float, default=40.0, help="nr-mix: LLR bytes the codeword counts are scaled to")
     ap.add_argument("--no-autotune", action="store_true", help="nr-mix: default launch shape")
     ap.add_argument("--learned-batch", type=int, default=65536)

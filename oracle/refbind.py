@@ -27,6 +27,16 @@ REF_DIR = os.path.join(HERE, "_ref")
 _u32p = C.POINTER(C.c_uint32)
 
 
+def _aligned(n: int, dtype, align: int = 64) -> np.ndarray:
+    """A zeroed 1-D array whose data starts on an `align`-byte boundary: the
+    reference's vector types are 32/64-byte aligned, and their stores may
+    assume it (its own buffers come from _mm_malloc)."""
+    itemsize = np.dtype(dtype).itemsize
+    raw = np.zeros(n * itemsize + align, np.uint8)
+    off = (-raw.ctypes.data) % align
+    return raw[off:off + n * itemsize].view(dtype)
+
+
 def ref_available(variant: str = "Vec64c_min") -> bool:
     return os.path.exists(os.path.join(REF_DIR, "libref_%s.so" % variant))
 
@@ -130,7 +140,9 @@ class RefCtx:
         self.lib.lib.ref_gen_rand_databits(self.h, self.num_cw)
 
     def gen_metrics(self, snr: float, wgn: np.ndarray, scale: float, max_abs: float) -> int:
-        wgn = np.ascontiguousarray(wgn, dtype=np.float32)
+        src = np.asarray(wgn, dtype=np.float32).ravel()
+        wgn = _aligned(src.size, np.float32)
+        wgn[:] = src
         return int(self.lib.lib.ref_gen_metrics(self.h, self.num_cw, snr,
                                                  wgn.ctypes.data_as(C.POINTER(C.c_float)), scale, max_abs))
 
@@ -152,7 +164,7 @@ def ref_init_randstate(lib: RefLib, seeds64) -> None:
 
 
 def ref_normdist2(lib: RefLib, simd_count: int) -> np.ndarray:
-    out = np.zeros(simd_count * 8, dtype=np.float32)
+    out = _aligned(simd_count * 8, np.float32)
     lib.lib.ref_normdist2(out.ctypes.data_as(C.POINTER(C.c_float)), simd_count)
     return out
 

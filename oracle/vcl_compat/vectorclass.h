@@ -16,7 +16,9 @@
  *   - permuteN<i...>() with index -1 yields zero;
  *   - mul_add() is a fused multiply-add.
  * Lane-generic C++ with AVX-512BW fast paths for the 64 x int8 operations
- * the decoder's inner loops use.  This is test infrastructure: nothing in
+ * the decoder's inner loops use, and AVX2 paths for the 32-byte vectors of
+ * the noise generator and gen_metrics (each the same wrap-around integer or
+ * correctly rounded float operation as the lane loop it replaces).  This is test infrastructure: nothing in
  * the shipped library includes it.
  */
 #ifndef VCL_COMPAT_VECTORCLASS_H
@@ -47,6 +49,46 @@ template <int N> struct VecB {
     friend VecB operator|(const VecB& a, const VecB& b) { VecB r; r.bits = a.bits | b.bits; return r; }
     friend VecB operator~(const VecB& a) { VecB r; r.bits = ~a.bits & all(); return r; }
 };
+
+#if defined(__AVX2__)
+/* 256-bit helpers for the 32-byte vectors (Vec8f/Vec8i/Vec4uq ...): the same
+ * wrap-around integer and correctly rounded float operations as the lane
+ * loops below. */
+static inline __m256i vclc_ld(const void* p) { return _mm256_loadu_si256((const __m256i*)p); }
+static inline void vclc_st(void* p, __m256i v) { _mm256_storeu_si256((__m256i*)p, v); }
+template <int B> static inline __m256i vclc_add(__m256i a, __m256i b) {
+    if constexpr (B == 1) return _mm256_add_epi8(a, b);
+    else if constexpr (B == 2) return _mm256_add_epi16(a, b);
+    else if constexpr (B == 4) return _mm256_add_epi32(a, b);
+    else return _mm256_add_epi64(a, b);
+}
+template <int B> static inline __m256i vclc_sub(__m256i a, __m256i b) {
+    if constexpr (B == 1) return _mm256_sub_epi8(a, b);
+    else if constexpr (B == 2) return _mm256_sub_epi16(a, b);
+    else if constexpr (B == 4) return _mm256_sub_epi32(a, b);
+    else return _mm256_sub_epi64(a, b);
+}
+/* shifts by a count >= 0; counts of the lane width or more give 0 (left,
+ * logical right) or the sign (arithmetic right), like the lane loops */
+template <int B> static inline __m256i vclc_sll(__m256i a, int s) {
+    const __m128i c = _mm_cvtsi32_si128(s);
+    if constexpr (B == 2) return _mm256_sll_epi16(a, c);
+    else if constexpr (B == 4) return _mm256_sll_epi32(a, c);
+    else return _mm256_sll_epi64(a, c);
+}
+template <int B, bool SIGNED> static inline __m256i vclc_sr(__m256i a, int s) {
+    const __m128i c = _mm_cvtsi32_si128(s);
+    if constexpr (!SIGNED) {
+        if constexpr (B == 2) return _mm256_srl_epi16(a, c);
+        else if constexpr (B == 4) return _mm256_srl_epi32(a, c);
+        else return _mm256_srl_epi64(a, c);
+    } else {
+        if constexpr (B == 2) return _mm256_sra_epi16(a, c);
+        else if constexpr (B == 4) return _mm256_sra_epi32(a, c);
+        else return _mm256_sra_epi64(a, c);   /* AVX-512VL */
+    }
+}
+#endif
 
 template <class T> struct sat_lim {
     static constexpr long long lo = std::is_signed<T>::value ? -(1LL << (8 * sizeof(T) - 1)) : 0;
@@ -109,17 +151,26 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
 #if defined(__AVX512F__)
         if constexpr (BYTES == 64) { Vec r; _mm512_storeu_si512(r.e, _mm512_and_si512(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r; }
 #endif
+#if defined(__AVX2__)
+        if constexpr (BYTES == 32) { Vec r; vclc_st(r.e, _mm256_and_si256(vclc_ld(a.e), vclc_ld(b.e))); return r; }
+#endif
         return bitop(a, b, [](unsigned char x, unsigned char y) { return (unsigned char)(x & y); });
     }
     friend Vec operator|(const Vec& a, const Vec& b) {
 #if defined(__AVX512F__)
         if constexpr (BYTES == 64) { Vec r; _mm512_storeu_si512(r.e, _mm512_or_si512(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r; }
 #endif
+#if defined(__AVX2__)
+        if constexpr (BYTES == 32) { Vec r; vclc_st(r.e, _mm256_or_si256(vclc_ld(a.e), vclc_ld(b.e))); return r; }
+#endif
         return bitop(a, b, [](unsigned char x, unsigned char y) { return (unsigned char)(x | y); });
     }
     friend Vec operator^(const Vec& a, const Vec& b) {
 #if defined(__AVX512F__)
         if constexpr (BYTES == 64) { Vec r; _mm512_storeu_si512(r.e, _mm512_xor_si512(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r; }
+#endif
+#if defined(__AVX2__)
+        if constexpr (BYTES == 32) { Vec r; vclc_st(r.e, _mm256_xor_si256(vclc_ld(a.e), vclc_ld(b.e))); return r; }
 #endif
         return bitop(a, b, [](unsigned char x, unsigned char y) { return (unsigned char)(x ^ y); });
     }
@@ -140,6 +191,10 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
         if constexpr (std::is_same<T, int8_t>::value && N == 64) { _mm512_storeu_si512(r.e, _mm512_add_epi8(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r; }
         if constexpr (std::is_same<T, float>::value && N == 16) { _mm512_storeu_ps(r.e, _mm512_add_ps(_mm512_loadu_ps(a.e), _mm512_loadu_ps(b.e))); return r; }
 #endif
+#if defined(__AVX2__)
+        if constexpr (BYTES == 32 && std::is_integral<T>::value) { vclc_st(r.e, vclc_add<sizeof(T)>(vclc_ld(a.e), vclc_ld(b.e))); return r; }
+        if constexpr (std::is_same<T, float>::value && N == 8) { _mm256_storeu_ps(r.e, _mm256_add_ps(_mm256_loadu_ps(a.e), _mm256_loadu_ps(b.e))); return r; }
+#endif
         if constexpr (std::is_integral<T>::value) {
             using U = typename std::make_unsigned<T>::type;
             for (int i = 0; i < N; ++i) r.e[i] = (T)(U)((U)a.e[i] + (U)b.e[i]);
@@ -154,6 +209,10 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
         if constexpr (std::is_same<T, int8_t>::value && N == 64) { _mm512_storeu_si512(r.e, _mm512_sub_epi8(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r; }
         if constexpr (std::is_same<T, float>::value && N == 16) { _mm512_storeu_ps(r.e, _mm512_sub_ps(_mm512_loadu_ps(a.e), _mm512_loadu_ps(b.e))); return r; }
 #endif
+#if defined(__AVX2__)
+        if constexpr (BYTES == 32 && std::is_integral<T>::value) { vclc_st(r.e, vclc_sub<sizeof(T)>(vclc_ld(a.e), vclc_ld(b.e))); return r; }
+        if constexpr (std::is_same<T, float>::value && N == 8) { _mm256_storeu_ps(r.e, _mm256_sub_ps(_mm256_loadu_ps(a.e), _mm256_loadu_ps(b.e))); return r; }
+#endif
         if constexpr (std::is_integral<T>::value) {
             using U = typename std::make_unsigned<T>::type;
             for (int i = 0; i < N; ++i) r.e[i] = (T)(U)((U)a.e[i] - (U)b.e[i]);
@@ -164,6 +223,9 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
     }
     friend Vec operator*(const Vec& a, const Vec& b) {
         Vec r;
+#if defined(__AVX2__)
+        if constexpr (std::is_same<T, float>::value && N == 8) { _mm256_storeu_ps(r.e, _mm256_mul_ps(_mm256_loadu_ps(a.e), _mm256_loadu_ps(b.e))); return r; }
+#endif
         if constexpr (std::is_integral<T>::value) {
             using U = typename std::make_unsigned<T>::type;
             for (int i = 0; i < N; ++i) r.e[i] = (T)(U)((U)a.e[i] * (U)b.e[i]);
@@ -179,11 +241,21 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
     Vec& operator*=(const Vec& b) { *this = *this * b; return *this; }
 
     friend Vec operator<<(const Vec& a, int s) {
+#if defined(__AVX2__)
+        if constexpr (BYTES == 32 && sizeof(T) >= 2 && std::is_integral<T>::value) {
+            if (s >= 0) { Vec r; vclc_st(r.e, vclc_sll<sizeof(T)>(vclc_ld(a.e), s)); return r; }
+        }
+#endif
         Vec r; using U = typename std::make_unsigned<T>::type;
         for (int i = 0; i < N; ++i) r.e[i] = (s >= (int)(8 * sizeof(T))) ? (T)0 : (T)(U)((U)a.e[i] << s);
         return r;
     }
     friend Vec operator>>(const Vec& a, int s) {
+#if defined(__AVX2__)
+        if constexpr (BYTES == 32 && sizeof(T) >= 2 && std::is_integral<T>::value) {
+            if (s >= 0) { Vec r; vclc_st(r.e, vclc_sr<sizeof(T), std::is_signed<T>::value>(vclc_ld(a.e), s)); return r; }
+        }
+#endif
         Vec r;
         for (int i = 0; i < N; ++i) {
             if (s >= (int)(8 * sizeof(T))) r.e[i] = std::is_signed<T>::value ? (T)(a.e[i] < 0 ? -1 : 0) : (T)0;
@@ -249,6 +321,13 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
             Vec r; _mm512_storeu_si512(r.e, _mm512_min_epi8(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r;
         }
 #endif
+#if defined(__AVX2__)
+        /* minps: the second operand unless the first compares less, as below */
+        if constexpr (std::is_same<T, float>::value && N == 8) { Vec r; _mm256_storeu_ps(r.e, _mm256_min_ps(_mm256_loadu_ps(a.e), _mm256_loadu_ps(b.e))); return r; }
+#endif
+#if defined(__AVX512F__)
+        if constexpr (std::is_same<T, float>::value && N == 16) { Vec r; _mm512_storeu_ps(r.e, _mm512_min_ps(_mm512_loadu_ps(a.e), _mm512_loadu_ps(b.e))); return r; }
+#endif
         Vec r; for (int i = 0; i < N; ++i) r.e[i] = (a.e[i] < b.e[i]) ? a.e[i] : b.e[i]; return r;
     }
     friend Vec max(const Vec& a, const Vec& b) {
@@ -256,6 +335,12 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
         if constexpr (std::is_same<T, int8_t>::value && N == 64) {
             Vec r; _mm512_storeu_si512(r.e, _mm512_max_epi8(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r;
         }
+#endif
+#if defined(__AVX2__)
+        if constexpr (std::is_same<T, float>::value && N == 8) { Vec r; _mm256_storeu_ps(r.e, _mm256_max_ps(_mm256_loadu_ps(a.e), _mm256_loadu_ps(b.e))); return r; }
+#endif
+#if defined(__AVX512F__)
+        if constexpr (std::is_same<T, float>::value && N == 16) { Vec r; _mm512_storeu_ps(r.e, _mm512_max_ps(_mm512_loadu_ps(a.e), _mm512_loadu_ps(b.e))); return r; }
 #endif
         Vec r; for (int i = 0; i < N; ++i) r.e[i] = (a.e[i] > b.e[i]) ? a.e[i] : b.e[i]; return r;
     }
@@ -302,6 +387,12 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
     }
     friend Vec mul_add(const Vec& a, const Vec& b, const Vec& c) {
         Vec r;
+#if defined(__AVX2__) && defined(__FMA__)
+        if constexpr (std::is_same<T, float>::value && N == 8) {
+            _mm256_storeu_ps(r.e, _mm256_fmadd_ps(_mm256_loadu_ps(a.e), _mm256_loadu_ps(b.e), _mm256_loadu_ps(c.e)));
+            return r;
+        }
+#endif
         if constexpr (std::is_same<T, float>::value) { for (int i = 0; i < N; ++i) r.e[i] = fmaf(a.e[i], b.e[i], c.e[i]); }
         else if constexpr (std::is_same<T, double>::value) { for (int i = 0; i < N; ++i) r.e[i] = fma(a.e[i], b.e[i], c.e[i]); }
         else { r = a * b + c; }
@@ -309,6 +400,9 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
     }
     friend Vec sqrt(const Vec& a) {
         Vec r;
+#if defined(__AVX2__)
+        if constexpr (std::is_same<T, float>::value && N == 8) { _mm256_storeu_ps(r.e, _mm256_sqrt_ps(_mm256_loadu_ps(a.e))); return r; }
+#endif
         if constexpr (std::is_same<T, float>::value) { for (int i = 0; i < N; ++i) r.e[i] = sqrtf(a.e[i]); }
         else { for (int i = 0; i < N; ++i) r.e[i] = (T)::sqrt((double)a.e[i]); }
         return r;
@@ -328,10 +422,25 @@ template <class T, int N> Raw<(int)sizeof(T) * N> reinterpret_f(const Vec<T, N>&
 template <int B> Raw<B> reinterpret_i(const Raw<B>& a) { return a; }
 template <int B> Raw<B> reinterpret_f(const Raw<B>& a) { return a; }
 
-template <int N> Vec<float, N> to_float(const Vec<int32_t, N>& a) { Vec<float, N> r; for (int i = 0; i < N; ++i) r.e[i] = (float)a.e[i]; return r; }
+template <int N> Vec<float, N> to_float(const Vec<int32_t, N>& a) {
+    Vec<float, N> r;
+#if defined(__AVX2__)
+    if constexpr (N == 8) { _mm256_storeu_ps(r.e, _mm256_cvtepi32_ps(vclc_ld(a.e))); return r; }
+#endif
+    for (int i = 0; i < N; ++i) r.e[i] = (float)a.e[i];
+    return r;
+}
 template <int N> Vec<float, N> to_float(const Vec<uint32_t, N>& a) { Vec<float, N> r; for (int i = 0; i < N; ++i) r.e[i] = (float)a.e[i]; return r; }
 template <int N> Vec<double, N> to_double(const Vec<float, N>& a) { Vec<double, N> r; for (int i = 0; i < N; ++i) r.e[i] = (double)a.e[i]; return r; }
-template <int N> Vec<int32_t, N> roundi(const Vec<float, N>& a) { Vec<int32_t, N> r; for (int i = 0; i < N; ++i) r.e[i] = (int32_t)nearbyintf(a.e[i]); return r; }
+template <int N> Vec<int32_t, N> roundi(const Vec<float, N>& a) {
+    Vec<int32_t, N> r;
+#if defined(__AVX2__)
+    /* cvtps2dq rounds by MXCSR (nearest-even by default), as nearbyintf does */
+    if constexpr (N == 8) { vclc_st(r.e, _mm256_cvtps_epi32(_mm256_loadu_ps(a.e))); return r; }
+#endif
+    for (int i = 0; i < N; ++i) r.e[i] = (int32_t)nearbyintf(a.e[i]);
+    return r;
+}
 template <int N> Vec<int32_t, N> truncatei(const Vec<float, N>& a) { Vec<int32_t, N> r; for (int i = 0; i < N; ++i) r.e[i] = (int32_t)a.e[i]; return r; }
 template <int N> Vec<int16_t, N> compress(const Vec<int32_t, N>& a) { Vec<int16_t, N> r; for (int i = 0; i < N; ++i) r.e[i] = (int16_t)(uint16_t)(uint32_t)a.e[i]; return r; }
 

@@ -1,6 +1,8 @@
-"""The reference's simulator input blob (run_LDPCsim.pl:79-82, read by
-read_sim_params.cpp:12-27) and the parse of its output lines
-(run_LDPCsim.pl:159-178), for the ldpc_sim tests."""
+"""The reference simulator's process protocol, for driving ldpc_sim (or an
+LDPCtop_* binary) from Python: the 820-byte stdin blob (run_LDPCsim.pl:79-82,
+read by read_sim_params.cpp:12-27), the parse of the output lines
+(run_LDPCsim.pl:159-178), and the generator key ldpc_sim folds from the 64
+seeds."""
 import re
 import struct
 

@@ -8,7 +8,7 @@ import subprocess
 import pytest
 
 from conftest import ROOT
-from simblob import blob, parse
+from ldpc_b200.simproto import blob, parse
 
 SIM = os.path.join(ROOT, "simd-fecfun_b200", "ldpc_b200", "ldpc_sim")
 

@@ -8,7 +8,7 @@ import subprocess
 import pytest
 
 from conftest import ROOT
-from simblob import blob, fold_seeds, parse
+from ldpc_b200.simproto import blob, fold_seeds, parse
 
 pytestmark = pytest.mark.gpu
 SIM = os.path.join(ROOT, "simd-fecfun_b200", "ldpc_b200", "ldpc_sim")
