@@ -195,6 +195,9 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
         if constexpr (BYTES == 32 && std::is_integral<T>::value) { vclc_st(r.e, vclc_add<sizeof(T)>(vclc_ld(a.e), vclc_ld(b.e))); return r; }
         if constexpr (std::is_same<T, float>::value && N == 8) { _mm256_storeu_ps(r.e, _mm256_add_ps(_mm256_loadu_ps(a.e), _mm256_loadu_ps(b.e))); return r; }
 #endif
+#if defined(__AVX512F__)
+        if constexpr (std::is_same<T, double>::value && N == 8) { _mm512_storeu_pd(r.e, _mm512_add_pd(_mm512_loadu_pd(a.e), _mm512_loadu_pd(b.e))); return r; }
+#endif
         if constexpr (std::is_integral<T>::value) {
             using U = typename std::make_unsigned<T>::type;
             for (int i = 0; i < N; ++i) r.e[i] = (T)(U)((U)a.e[i] + (U)b.e[i]);
@@ -213,6 +216,9 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
         if constexpr (BYTES == 32 && std::is_integral<T>::value) { vclc_st(r.e, vclc_sub<sizeof(T)>(vclc_ld(a.e), vclc_ld(b.e))); return r; }
         if constexpr (std::is_same<T, float>::value && N == 8) { _mm256_storeu_ps(r.e, _mm256_sub_ps(_mm256_loadu_ps(a.e), _mm256_loadu_ps(b.e))); return r; }
 #endif
+#if defined(__AVX512F__)
+        if constexpr (std::is_same<T, double>::value && N == 8) { _mm512_storeu_pd(r.e, _mm512_sub_pd(_mm512_loadu_pd(a.e), _mm512_loadu_pd(b.e))); return r; }
+#endif
         if constexpr (std::is_integral<T>::value) {
             using U = typename std::make_unsigned<T>::type;
             for (int i = 0; i < N; ++i) r.e[i] = (T)(U)((U)a.e[i] - (U)b.e[i]);
@@ -225,6 +231,10 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
         Vec r;
 #if defined(__AVX2__)
         if constexpr (std::is_same<T, float>::value && N == 8) { _mm256_storeu_ps(r.e, _mm256_mul_ps(_mm256_loadu_ps(a.e), _mm256_loadu_ps(b.e))); return r; }
+#endif
+#if defined(__AVX512F__)
+        if constexpr (std::is_same<T, float>::value && N == 16) { _mm512_storeu_ps(r.e, _mm512_mul_ps(_mm512_loadu_ps(a.e), _mm512_loadu_ps(b.e))); return r; }
+        if constexpr (std::is_same<T, double>::value && N == 8) { _mm512_storeu_pd(r.e, _mm512_mul_pd(_mm512_loadu_pd(a.e), _mm512_loadu_pd(b.e))); return r; }
 #endif
         if constexpr (std::is_integral<T>::value) {
             using U = typename std::make_unsigned<T>::type;
@@ -327,6 +337,7 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
 #endif
 #if defined(__AVX512F__)
         if constexpr (std::is_same<T, float>::value && N == 16) { Vec r; _mm512_storeu_ps(r.e, _mm512_min_ps(_mm512_loadu_ps(a.e), _mm512_loadu_ps(b.e))); return r; }
+        if constexpr (std::is_same<T, double>::value && N == 8) { Vec r; _mm512_storeu_pd(r.e, _mm512_min_pd(_mm512_loadu_pd(a.e), _mm512_loadu_pd(b.e))); return r; }
 #endif
         Vec r; for (int i = 0; i < N; ++i) r.e[i] = (a.e[i] < b.e[i]) ? a.e[i] : b.e[i]; return r;
     }
@@ -341,6 +352,7 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
 #endif
 #if defined(__AVX512F__)
         if constexpr (std::is_same<T, float>::value && N == 16) { Vec r; _mm512_storeu_ps(r.e, _mm512_max_ps(_mm512_loadu_ps(a.e), _mm512_loadu_ps(b.e))); return r; }
+        if constexpr (std::is_same<T, double>::value && N == 8) { Vec r; _mm512_storeu_pd(r.e, _mm512_max_pd(_mm512_loadu_pd(a.e), _mm512_loadu_pd(b.e))); return r; }
 #endif
         Vec r; for (int i = 0; i < N; ++i) r.e[i] = (a.e[i] > b.e[i]) ? a.e[i] : b.e[i]; return r;
     }
@@ -355,6 +367,13 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
             using U = typename std::make_unsigned<T>::type;
             for (int i = 0; i < N; ++i) r.e[i] = (a.e[i] < 0) ? (T)(U)(0u - (U)a.e[i]) : a.e[i];
         } else {
+#if defined(__AVX512F__)
+            if constexpr (BYTES == 64) {   /* fabs: clear the sign bits */
+                const __m512i m = sizeof(T) == 4 ? _mm512_set1_epi32(0x7fffffff) : _mm512_set1_epi64(0x7fffffffffffffffLL);
+                _mm512_storeu_si512(r.e, _mm512_and_si512(_mm512_loadu_si512(a.e), m));
+                return r;
+            }
+#endif
             for (int i = 0; i < N; ++i) r.e[i] = fabs(a.e[i]);
         }
         return r;
@@ -390,6 +409,16 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
 #if defined(__AVX2__) && defined(__FMA__)
         if constexpr (std::is_same<T, float>::value && N == 8) {
             _mm256_storeu_ps(r.e, _mm256_fmadd_ps(_mm256_loadu_ps(a.e), _mm256_loadu_ps(b.e), _mm256_loadu_ps(c.e)));
+            return r;
+        }
+#endif
+#if defined(__AVX512F__)
+        if constexpr (std::is_same<T, float>::value && N == 16) {
+            _mm512_storeu_ps(r.e, _mm512_fmadd_ps(_mm512_loadu_ps(a.e), _mm512_loadu_ps(b.e), _mm512_loadu_ps(c.e)));
+            return r;
+        }
+        if constexpr (std::is_same<T, double>::value && N == 8) {
+            _mm512_storeu_pd(r.e, _mm512_fmadd_pd(_mm512_loadu_pd(a.e), _mm512_loadu_pd(b.e), _mm512_loadu_pd(c.e)));
             return r;
         }
 #endif
@@ -489,6 +518,13 @@ typedef vclc::VecB<64> Vec64cb;
  * vectorclass_extensions.h). */
 template <class V> static inline V vclc_sign_combine_f(const V& a, const V& b) {
     V r;
+#if defined(__AVX512F__)
+    if constexpr (V::BYTES == 64) {   /* a with its sign bit flipped where b's is set: a ^ (b & sign) */
+        const __m512i m = sizeof(a.e[0]) == 4 ? _mm512_set1_epi32((int)0x80000000u) : _mm512_set1_epi64((long long)0x8000000000000000ULL);
+        _mm512_storeu_si512(r.e, _mm512_xor_si512(_mm512_loadu_si512(a.e), _mm512_and_si512(_mm512_loadu_si512(b.e), m)));
+        return r;
+    }
+#endif
     for (int i = 0; i < V::size(); ++i) r.e[i] = std::signbit(b.e[i]) ? -a.e[i] : a.e[i];
     return r;
 }
