@@ -90,6 +90,20 @@ template <int B, bool SIGNED> static inline __m256i vclc_sr(__m256i a, int s) {
 }
 #endif
 
+#if defined(__AVX512F__)
+/* saturating 32-bit add (sub = true: a - b): the wrapped result, replaced by
+ * INT32_MIN / INT32_MAX (by the sign of a) where the operation overflowed */
+static inline __m512i vclc_sat32(__m512i a, __m512i b, bool sub) {
+    const __m512i r = sub ? _mm512_sub_epi32(a, b) : _mm512_add_epi32(a, b);
+    /* overflow: add -- a, b same sign and r differs; sub -- a, b differ and r differs from a */
+    const __m512i ov = sub ? _mm512_and_si512(_mm512_xor_si512(a, b), _mm512_xor_si512(a, r))
+                           : _mm512_andnot_si512(_mm512_xor_si512(a, b), _mm512_xor_si512(a, r));
+    const __mmask16 m = _mm512_movepi32_mask(ov);
+    const __m512i lim = _mm512_xor_si512(_mm512_srai_epi32(a, 31), _mm512_set1_epi32(0x7fffffff));
+    return _mm512_mask_blend_epi32(m, r, lim);
+}
+#endif
+
 template <class T> struct sat_lim {
     static constexpr long long lo = std::is_signed<T>::value ? -(1LL << (8 * sizeof(T) - 1)) : 0;
     static constexpr long long hi = std::is_signed<T>::value ? (1LL << (8 * sizeof(T) - 1)) - 1
@@ -189,6 +203,8 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
         Vec r;
 #if defined(__AVX512BW__)
         if constexpr (std::is_same<T, int8_t>::value && N == 64) { _mm512_storeu_si512(r.e, _mm512_add_epi8(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r; }
+        if constexpr (std::is_same<T, int16_t>::value && N == 32) { _mm512_storeu_si512(r.e, _mm512_add_epi16(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r; }
+        if constexpr (std::is_same<T, int32_t>::value && N == 16) { _mm512_storeu_si512(r.e, _mm512_add_epi32(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r; }
         if constexpr (std::is_same<T, float>::value && N == 16) { _mm512_storeu_ps(r.e, _mm512_add_ps(_mm512_loadu_ps(a.e), _mm512_loadu_ps(b.e))); return r; }
 #endif
 #if defined(__AVX2__)
@@ -210,6 +226,8 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
         Vec r;
 #if defined(__AVX512BW__)
         if constexpr (std::is_same<T, int8_t>::value && N == 64) { _mm512_storeu_si512(r.e, _mm512_sub_epi8(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r; }
+        if constexpr (std::is_same<T, int16_t>::value && N == 32) { _mm512_storeu_si512(r.e, _mm512_sub_epi16(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r; }
+        if constexpr (std::is_same<T, int32_t>::value && N == 16) { _mm512_storeu_si512(r.e, _mm512_sub_epi32(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r; }
         if constexpr (std::is_same<T, float>::value && N == 16) { _mm512_storeu_ps(r.e, _mm512_sub_ps(_mm512_loadu_ps(a.e), _mm512_loadu_ps(b.e))); return r; }
 #endif
 #if defined(__AVX2__)
@@ -330,6 +348,12 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
         if constexpr (std::is_same<T, int8_t>::value && N == 64) {
             Vec r; _mm512_storeu_si512(r.e, _mm512_min_epi8(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r;
         }
+        if constexpr (std::is_same<T, int16_t>::value && N == 32) {
+            Vec r; _mm512_storeu_si512(r.e, _mm512_min_epi16(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r;
+        }
+        if constexpr (std::is_same<T, int32_t>::value && N == 16) {
+            Vec r; _mm512_storeu_si512(r.e, _mm512_min_epi32(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r;
+        }
 #endif
 #if defined(__AVX2__)
         /* minps: the second operand unless the first compares less, as below */
@@ -345,6 +369,12 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
 #if defined(__AVX512BW__)
         if constexpr (std::is_same<T, int8_t>::value && N == 64) {
             Vec r; _mm512_storeu_si512(r.e, _mm512_max_epi8(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r;
+        }
+        if constexpr (std::is_same<T, int16_t>::value && N == 32) {
+            Vec r; _mm512_storeu_si512(r.e, _mm512_max_epi16(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r;
+        }
+        if constexpr (std::is_same<T, int32_t>::value && N == 16) {
+            Vec r; _mm512_storeu_si512(r.e, _mm512_max_epi32(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r;
         }
 #endif
 #if defined(__AVX2__)
@@ -362,6 +392,12 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
 #if defined(__AVX512BW__)
             if constexpr (std::is_same<T, int8_t>::value && N == 64) {
                 _mm512_storeu_si512(r.e, _mm512_abs_epi8(_mm512_loadu_si512(a.e))); return r;
+            }
+            if constexpr (std::is_same<T, int16_t>::value && N == 32) {
+                _mm512_storeu_si512(r.e, _mm512_abs_epi16(_mm512_loadu_si512(a.e))); return r;
+            }
+            if constexpr (std::is_same<T, int32_t>::value && N == 16) {
+                _mm512_storeu_si512(r.e, _mm512_abs_epi32(_mm512_loadu_si512(a.e))); return r;
             }
 #endif
             using U = typename std::make_unsigned<T>::type;
@@ -383,6 +419,12 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
         if constexpr (std::is_same<T, int8_t>::value && N == 64) {
             Vec r; _mm512_storeu_si512(r.e, _mm512_adds_epi8(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r;
         }
+        if constexpr (std::is_same<T, int16_t>::value && N == 32) {
+            Vec r; _mm512_storeu_si512(r.e, _mm512_adds_epi16(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r;
+        }
+        if constexpr (std::is_same<T, int32_t>::value && N == 16) {
+            Vec r; _mm512_storeu_si512(r.e, vclc_sat32(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e), false)); return r;
+        }
 #endif
         Vec r;
         for (int i = 0; i < N; ++i) {
@@ -395,6 +437,12 @@ struct alignas((sizeof(T) * N) >= 64 ? 64 : (sizeof(T) * N)) Vec {
 #if defined(__AVX512BW__)
         if constexpr (std::is_same<T, int8_t>::value && N == 64) {
             Vec r; _mm512_storeu_si512(r.e, _mm512_subs_epi8(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r;
+        }
+        if constexpr (std::is_same<T, int16_t>::value && N == 32) {
+            Vec r; _mm512_storeu_si512(r.e, _mm512_subs_epi16(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e))); return r;
+        }
+        if constexpr (std::is_same<T, int32_t>::value && N == 16) {
+            Vec r; _mm512_storeu_si512(r.e, vclc_sat32(_mm512_loadu_si512(a.e), _mm512_loadu_si512(b.e), true)); return r;
         }
 #endif
         Vec r;
