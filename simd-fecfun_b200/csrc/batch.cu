@@ -177,14 +177,14 @@ int float_plan(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int thread
         return m;
     };
     if (rsmem && prod) {
-        // as for a single code: sum-product keeps shared-memory messages only
-        // when they keep as many CTAs per SM as global (L2) messages
+        // as for a single code: sum-product keeps shared-memory messages
+        // unless global (L2) messages give at least 1.5 times the CTAs per SM
         int per_s = 0, per_g = 0;
         CUDA_TRY(ldpc::allow_dynamic_smem((const void*)find(true), ldpc::kSpMaxSmem));
         CUDA_TRY(ldpc::allow_dynamic_smem((const void*)find(false), ldpc::kSpMaxSmem));
         CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_s, (const void*)find(true), threads, smem_of(true)));
         CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_g, (const void*)find(false), threads, smem_of(false)));
-        rsmem = per_s >= per_g;
+        rsmem = 2 * per_g < 3 * per_s;
     }
     const size_t smem = smem_of(rsmem);
     spb_fn k = find(rsmem);

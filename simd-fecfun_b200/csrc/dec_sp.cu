@@ -79,11 +79,12 @@ int setup_sp(ldpc_ctx* x) {
     t.nostage = nostage ? 1 : 0;
     x->sp_threads = ((G * c.z + 31) / 32) * 32;
     const size_t r_smem = (size_t)t.E * x->sp_threads * es;
-    // sum-product: messages in shared memory only when that keeps as many
-    // CTAs per SM as messages in global scratch (L2) would -- its tanh/atanh
+    // sum-product: messages in shared memory unless messages in global
+    // scratch (L2) give at least 1.5 times the CTAs per SM -- its tanh/atanh
     // chains are latency-bound, so resident warps count for more than
-    // message latency.  Min-sum, light on arithmetic, keeps them in shared
-    // memory whenever they fit.
+    // message latency, but one CTA more out of five does not pay for the L2
+    // round trips (802.11ad float: 6 vs 5 CTAs is 5 % slower).  Min-sum,
+    // light on arithmetic, keeps them in shared memory whenever they fit.
     auto find = [&](bool rs) {
         const SpVariant* f = nullptr;
         for (const SpVariant& k : kSp)
@@ -103,7 +104,7 @@ int setup_sp(ldpc_ctx* x) {
         int per_s = 0, per_g = 0;
         CUDA_TRY(ctas_per_sm(find(true), base_smem + r_smem, &per_s));
         CUDA_TRY(ctas_per_sm(find(false), base_smem, &per_g));
-        rsmem = !prod || per_s >= per_g || getenv("LDPC_SP_RSMEM");
+        rsmem = !prod || 2 * per_g < 3 * per_s || getenv("LDPC_SP_RSMEM");
     }
     const SpVariant* v = find(rsmem);
     x->sp_kernel = dbl ? nullptr : v->k;

@@ -42,7 +42,7 @@ struct SpBatchLaunch {
 __host__ __device__ constexpr int sp_code_bytes() { return (int)((sizeof(SpCode) + 15) & ~(size_t)15); }
 
 template <int DMAX, bool PROD, bool RSMEM>
-__global__ void __launch_bounds__(512) sp_batch_kernel(const __grid_constant__ SpBatchLaunch lp) {
+__global__ void __maxnreg__(sp_max_regs(DMAX, PROD, RSMEM)) sp_batch_kernel(const __grid_constant__ SpBatchLaunch lp) {
     extern __shared__ __align__(16) unsigned char spb_smem[];
     __shared__ int s_code;
     const SpCode& C = *reinterpret_cast<const SpCode*>(spb_smem);

@@ -280,8 +280,17 @@ __device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJobT
     }
 }
 
+// Register budget of a float kernel instance.  Sum-product on rows of weight
+// <= 8 with its check messages in global scratch is held to 80 registers
+// (no spills): 128-thread CTAs then fit 6 per SM instead of 5 and 384-thread
+// CTAs 2 instead of 1, which pays in this latency-bound case (tanh/atanh
+// chains).  Every other instance keeps the 128 that a 512-thread CTA allows.
+__host__ __device__ constexpr int sp_max_regs(int dmax, bool prod, bool rsmem) {
+    return dmax == 8 && prod && !rsmem ? 80 : 128;
+}
+
 template <int DMAX, bool PROD, bool RSMEM, int MAXT>
-__global__ void __launch_bounds__(MAXT) sp_f32_kernel(const __grid_constant__ SpTables tb, const __grid_constant__ SpJob job) {
+__global__ void __maxnreg__(sp_max_regs(DMAX, PROD, RSMEM)) sp_f32_kernel(const __grid_constant__ SpTables tb, const __grid_constant__ SpJob job) {
     extern __shared__ __align__(16) float sm_f[];
     const long long lo = job.ncw * blockIdx.x / gridDim.x, hi = job.ncw * (blockIdx.x + 1) / gridDim.x;
     sp_decode_range<DMAX, PROD, RSMEM>(tb, job, lo, hi, sm_f,
