@@ -19,8 +19,8 @@ const int kRw11ad12[] = {5, 6, 6, 6, 7, 7, 7, 8};
 #define OMS_COMPILED(C_, RW_) {C_::L, C_::D, RW_, &kCompiled##C_, 0, 4, {OMS_K(CompiledShape<C_>, 640, 1), OMS_K(CompiledShape<C_>, 256, 2), OMS_K(CompiledShape<C_>, 192, 3), OMS_K(CompiledShape<C_>, 128, 5)}}
 #define OMS_SPLIT(C_, RW_, EREG_)                                                                           \
     {C_::L, C_::D, RW_, &kCompiled##C_, C_::E - EREG_, 2,                                                    \
-     {{128, 7, oms_f16_kernel<SplitShape<C_, EREG_>, false, 128, 7>, oms_f16_kernel<SplitShape<C_, EREG_>, true, 128, 7>}, \
-      {96, 8, oms_f16_kernel<SplitShape<C_, EREG_>, false, 96, 8>, oms_f16_kernel<SplitShape<C_, EREG_>, true, 96, 8>}}}
+     {{128, 7, oms_f16_kernel<SplitShape<C_, EREG_, 128>, false, 128, 7>, oms_f16_kernel<SplitShape<C_, EREG_, 128>, true, 128, 7>}, \
+      {96, 8, oms_f16_kernel<SplitShape<C_, EREG_, 96>, false, 96, 8>, oms_f16_kernel<SplitShape<C_, EREG_, 96>, true, 96, 8>}}}
 #define OMS_PAD(L_, D_) {L_, D_, nullptr, nullptr, 0, 1, {{384, 1, oms_f16_kernel<PaddedShape<L_, D_>, false, 384, 1>, oms_f16_kernel<PaddedShape<L_, D_>, true, 384, 1>}}}
 // compiled-in code descriptions (columns, shifts) for table matching
 template <class C>
@@ -145,9 +145,9 @@ int setup_oms(ldpc_ctx* x) {
     t.G = G;
     t.stride = stride;
     x->oms_threads = ((G * c.z + 31) / 32) * 32;
-    x->oms_threads = ((G * c.z + 31) / 32) * 32;
-    // posteriors + LLR staging + shared-memory check messages
-    x->oms_smem = ((G * stride * 4 + 15) & ~15) + 2 * G * ((t.n + 15) & ~15) + best->smem_edges * x->oms_threads * 4;
+    // posteriors + LLR staging + shared-memory check messages (strided by
+    // the launch's maximum CTA size, a compile-time constant of the kernel)
+    x->oms_smem = ((G * stride * 4 + 15) & ~15) + 2 * G * ((t.n + 15) & ~15) + best->smem_edges * lv->max_threads * 4;
     if (x->oms_smem > kOmsMaxSmem) return fail(LDPC_ERR_UNSUPPORTED, "int8 decoder: %d B of shared memory", x->oms_smem);
     CUDA_TRY(allow_dynamic_smem((const void*)k, kOmsMaxSmem));
     int per_sm = 0;

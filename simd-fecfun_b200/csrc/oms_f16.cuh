@@ -93,6 +93,7 @@ struct FixedShape {
     static constexpr int L = sizeof...(RW);
     static constexpr int E = (RW + ...);
     static constexpr int E_REG = E;
+    static constexpr int RS_STRIDE = 0;
     static constexpr int D = [] { int m = 0; for (int v : {RW...}) m = v > m ? v : m; return m; }();
     __host__ __device__ static constexpr int maxd(int l) {
         constexpr int rw[] = {RW...};
@@ -119,6 +120,7 @@ struct CompiledShape {
     static constexpr int L = C::L;
     static constexpr int E = C::E;
     static constexpr int E_REG = C::E;
+    static constexpr int RS_STRIDE = 0;
     static constexpr int D = C::D;
     __host__ __device__ static constexpr int maxd(int l) { return C::maxd(l); }
     __host__ __device__ static constexpr int slot(int l, int j) { return C::slot(l, j); }
@@ -130,10 +132,13 @@ struct CompiledShape {
 };
 
 // Compiled code with the check messages of edge slots >= EREG kept in shared
-// memory instead of registers (fewer registers, more resident warps).
-template <class C, int EREG>
+// memory instead of registers (fewer registers, more resident warps).  They
+// sit at Rs[(e - EREG) * NT + tid], NT = the launch's maximum CTA size, so
+// every such address is the thread's base plus an immediate.
+template <class C, int EREG, int NT>
 struct SplitShape : CompiledShape<C> {
     static constexpr int E_REG = EREG;
+    static constexpr int RS_STRIDE = NT;
 };
 
 template <int L_, int D_>
@@ -142,6 +147,7 @@ struct PaddedShape {
     static constexpr int D = D_;
     static constexpr int E = L_ * D_;
     static constexpr int E_REG = E;
+    static constexpr int RS_STRIDE = 0;
     __host__ __device__ static constexpr int maxd(int) { return D_; }
     __host__ __device__ static constexpr int slot(int l, int j) { return l * D_ + j; }
     __device__ static bool has(const OmsTables& tb, int l, int j) {
@@ -157,18 +163,18 @@ struct PaddedShape {
 
 struct OmsConsts {
     uint32_t beta2, maxv2;
-    uint32_t* Rs;        // shared-memory messages of edge slots >= E_REG: Rs[(e - E_REG) * nthreads]
+    uint32_t* Rs;        // shared-memory messages of edge slots >= E_REG: Rs[(e - E_REG) * S::RS_STRIDE]
 };
 
 template <class S>
 __device__ __forceinline__ uint32_t get_r(const uint32_t (&R)[S::E_REG > 0 ? S::E_REG : 1], const OmsConsts& k, int e) {
     if (e < S::E_REG) return R[e < S::E_REG ? e : 0];
-    return k.Rs[(e - S::E_REG) * blockDim.x];
+    return k.Rs[(e - S::E_REG) * S::RS_STRIDE];
 }
 template <class S>
 __device__ __forceinline__ void set_r(uint32_t (&R)[S::E_REG > 0 ? S::E_REG : 1], const OmsConsts& k, int e, uint32_t v) {
     if (e < S::E_REG) R[e < S::E_REG ? e : 0] = v;
-    else k.Rs[(e - S::E_REG) * blockDim.x] = v;
+    else k.Rs[(e - S::E_REG) * S::RS_STRIDE] = v;
 }
 
 // One layer of the layered update for this thread's check row t (all edges
@@ -389,7 +395,7 @@ __global__ void __launch_bounds__(MAXT, MINB) oms_f16_kernel(const __grid_consta
     kc.maxv2 = job.maxv2;
     // shared-memory messages after the LLR staging area
     kc.Rs = reinterpret_cast<uint32_t*>(stage_base + 2 * G * nstage) + tid;
-    for (int e = S::E_REG; e < S::E; ++e) kc.Rs[(e - S::E_REG) * blockDim.x] = 0u;
+    for (int e = S::E_REG; e < S::E; ++e) kc.Rs[(e - S::E_REG) * S::RS_STRIDE] = 0u;
 
     for (int par = 0;; par ^= 1) {
         // ================= one layered iteration =================
@@ -497,7 +503,7 @@ __global__ void __launch_bounds__(MAXT, MINB) oms_f16_kernel(const __grid_consta
             if (m) {
 #pragma unroll
                 for (int e = 0; e < S::E_REG; ++e) R[e] &= ~m;
-                for (int e = S::E_REG; e < S::E; ++e) kc.Rs[(e - S::E_REG) * blockDim.x] &= ~m;
+                for (int e = S::E_REG; e < S::E; ++e) kc.Rs[(e - S::E_REG) * S::RS_STRIDE] &= ~m;
             }
         }
         if (!s_busy[par]) break;
