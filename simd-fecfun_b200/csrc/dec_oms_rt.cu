@@ -38,7 +38,7 @@ int rt_stride(int n, int G) {
 size_t rt_smem_bytes(int n, int G, int E, int threads, bool rsmem) {
     const size_t nstage = (size_t)((n + 15) & ~15);
     return (size_t)rt_code_bytes() + (((size_t)G * rt_stride(n, G) * 4 + 15) & ~(size_t)15) + 2 * (size_t)G * nstage +
-           (rsmem ? (size_t)E * threads * 4 : 0);
+           (rsmem ? (size_t)(E | 1) * threads * 4 : 0);   // odd per-thread stride
 }
 
 int rt_dmax(int d) { return d <= 8 ? 8 : d <= 12 ? 12 : d <= 16 ? 16 : d <= 24 ? 24 : d <= 32 ? 32 : 0; }

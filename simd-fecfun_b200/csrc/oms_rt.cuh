@@ -35,7 +35,7 @@ __device__ __forceinline__ void rt_offsets(const RtCode& C, int l, int it0, int 
 }
 
 template <int DMAX, bool QUIRK>
-__device__ __forceinline__ void rt_layer(const RtCode& C, int l, uint32_t* Ps, uint32_t* Rt, int nthr, int t, int gbase,
+__device__ __forceinline__ void rt_layer(const RtCode& C, int l, uint32_t* Ps, uint32_t* Rt, int rstride, int t, int gbase,
                                          int z, uint32_t beta2, uint32_t quirk_l) {
     constexpr uint32_t SGN = 0x80008000u;
     const int d = C.rw[l], eb = C.ebase[l];
@@ -49,7 +49,7 @@ __device__ __forceinline__ void rt_layer(const RtCode& C, int l, uint32_t* Ps, u
         if (j < d) {
             const uint32_t ed = C.edge[eb + j];
             addr[j] = gbase + (int)(ed >> 9) + wrap_add(t, (int)(ed & 511u), z);
-            uint32_t Q = hsub2(Ps[addr[j]], Rt[(eb + j) * nthr]);
+            uint32_t Q = hsub2(Ps[addr[j]], Rt[(eb + j) * rstride]);
             Q = hmin2(hmax2(Q, H2_M128), H2_P127);
             if (QUIRK) {
                 uint32_t a = habs2(Q);
@@ -82,7 +82,7 @@ __device__ __forceinline__ void rt_layer(const RtCode& C, int l, uint32_t* Ps, u
             const uint32_t Rn = M1 ^ (q[j] & SGN) ^ (eq & X);
             const uint32_t Pn = hmin2(hmax2(hadd2(q[j], Rn), H2_M128), H2_P127);
             Ps[addr[j]] = Pn;
-            Rt[(eb + j) * nthr] = Rn;
+            Rt[(eb + j) * rstride] = Rn;
         }
     }
 }
@@ -135,7 +135,7 @@ __device__ __forceinline__ void rt_syndrome(const RtCode& C, const uint32_t* Ps,
     }
 }
 
-// Shared memory: [RtCode copy][posteriors G x stride words][LLR staging 2G x nstage bytes][messages E x blockDim words if RSMEM]
+// Shared memory: [RtCode copy][posteriors G x stride words][LLR staging 2G x nstage bytes][messages (E | 1) x blockDim words if RSMEM]
 __host__ __device__ constexpr int rt_code_bytes() { return (int)((sizeof(RtCode) + 15) & ~(size_t)15); }
 
 template <int DMAX, bool QUIRK, bool RSMEM>
@@ -197,12 +197,17 @@ __global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtL
         const int t = tid / G, g = tid - (tid / G) * G;
         const bool active = t < z;
         const int gbase = g * stride;
-        uint32_t* const Rt = RSMEM ? reinterpret_cast<uint32_t*>(stage_base + 2 * G * nstage) + tid
+        // check messages: in shared memory each thread's E words are contiguous
+        // at an odd stride (E | 1, so a warp's 32 lanes fall in 32 banks) and
+        // edge j of a layer is the layer's base plus an immediate; the global
+        // scratch keeps edge-major words (coalesced)
+        const int rstride = RSMEM ? 1 : nthr;
+        uint32_t* const Rt = RSMEM ? reinterpret_cast<uint32_t*>(stage_base + 2 * G * nstage) + tid * (E | 1)
                                    : lp.r_scratch + (long long)blockIdx.x * lp.r_words_per_cta + tid;
 
         for (int i = tid; i < OMS_MAX_BUCKETS * 4; i += nthr) (&s_cnt[0][0])[i] = 0;
         for (int i = tid; i < G * stride; i += nthr) Ps[i] = 0;
-        for (int e = 0; e < E; ++e) Rt[e * nthr] = 0u;
+        for (int e = 0; e < E; ++e) Rt[e * rstride] = 0u;
         if (tid < 32) {
             const long long c0 = lo + tid, c1 = lo + nslots + tid;
             const bool ok = tid < nslots;
@@ -238,7 +243,7 @@ __global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtL
                     uint32_t beta2, quirk;
                     rt_offsets(C, l, it0, it1, beta2, quirk);
                     rt_dispatch<DMAX>(C.rw[l], [&](auto D) {
-                        rt_layer<decltype(D)::value, QUIRK>(C, l, Ps, Rt, nthr, t, gbase, z, beta2, quirk);
+                        rt_layer<decltype(D)::value, QUIRK>(C, l, Ps, Rt, rstride, t, gbase, z, beta2, quirk);
                     });
                 }
                 __syncthreads();
@@ -334,7 +339,7 @@ __global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtL
             if (active) {
                 const uint32_t m = s_zero_mask[par][g];
                 if (m)
-                    for (int e = 0; e < E; ++e) Rt[e * nthr] &= ~m;
+                    for (int e = 0; e < E; ++e) Rt[e * rstride] &= ~m;
             }
             if (!s_busy[par]) break;
         }
