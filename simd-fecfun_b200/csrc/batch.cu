@@ -160,7 +160,7 @@ int float_plan(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int thread
         base[c] = bytes(G[c]);
         if (base[c] > (size_t)ldpc::kSpMaxSmem)
             return fail(LDPC_ERR_UNSUPPORTED, "batch plan: code %d (N=%d) does not fit shared memory", c, n);
-        if (base[c] + (size_t)E * threads * 4 > (size_t)ldpc::kSpMaxSmem) rsmem = false;
+        if (base[c] + (size_t)(E | 1) * threads * 4 > (size_t)ldpc::kSpMaxSmem) rsmem = false;   // odd per-thread stride
         dmax = std::max(dmax, cd.max_row_weight <= 8 ? 8 : cd.max_row_weight <= 16 ? 16 : 32);
         maxE = std::max(maxE, E);
     }
@@ -173,7 +173,7 @@ int float_plan(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, int thread
     auto smem_of = [&](bool rs) {
         size_t m = 0;
         for (int c = 0; c < nc; ++c)
-            if (used[c]) m = std::max(m, base[c] + (rs ? (size_t)b->codes[c].row_cols.size() * threads * 4 : 0));
+            if (used[c]) m = std::max(m, base[c] + (rs ? (size_t)((int)b->codes[c].row_cols.size() | 1) * threads * 4 : 0));
         return m;
     };
     if (rsmem && prod) {

@@ -78,7 +78,10 @@ int setup_sp(ldpc_ctx* x) {
     const size_t base_smem = base_bytes(G, !nostage);   // leaves t filled for G
     t.nostage = nostage ? 1 : 0;
     x->sp_threads = ((G * c.z + 31) / 32) * 32;
-    const size_t r_smem = (size_t)t.E * x->sp_threads * es;
+    // messages: shared memory holds E | 1 per thread (odd stride), the global
+    // scratch E per thread
+    const size_t r_smem = (size_t)(t.E | 1) * x->sp_threads * es;
+    const size_t r_glob = (size_t)t.E * x->sp_threads * es;
     // sum-product: messages in shared memory unless messages in global
     // scratch (L2) give at least 1.5 times the CTAs per SM -- its tanh/atanh
     // chains are latency-bound, so resident warps count for more than
@@ -120,7 +123,7 @@ int setup_sp(ldpc_ctx* x) {
     if (per_sm < 1) return fail(LDPC_ERR_UNSUPPORTED, "float decoder: launch does not fit an SM");
     x->sp_ctas = per_sm * x->sms;
     if (!rsmem) {
-        CUDA_TRY(cudaMalloc(&x->d_sp_scratch, (size_t)x->sp_ctas * r_smem));
+        CUDA_TRY(cudaMalloc(&x->d_sp_scratch, (size_t)x->sp_ctas * r_glob));
     }
     // decode_row's Max_row_simd (decode_functions.cpp:27-32): 1 - (CTYPE)max_row_metric
     // below 1e-6 (sum-product), else max_row_metric, in the build's element type

@@ -111,12 +111,17 @@ __device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJobT
     T* stage = sm_f + ((G * stride + V - 1) & ~(V - 1));            // [G][nstage], 16-byte aligned
     const int nstage = (n + V - 1) & ~(V - 1);
     T* Rbase = RSMEM ? stage + (staged ? G * nstage : 0) : r_cta;
-    T* Rt = Rbase + tid;                                            // message of edge e at Rt[e * nthr]
+    // check messages: in shared memory each thread's E values are contiguous
+    // at an odd stride (E | 1: a warp's lanes fall in distinct banks), so edge
+    // e is the thread's base plus e; the global scratch keeps edge-major
+    // values (coalesced), edge e at Rt[e * nthr]
+    const int rstride = RSMEM ? 1 : nthr;
+    T* Rt = RSMEM ? Rbase + tid * (tb.E | 1) : Rbase + tid;
     const T beta = job.beta, maxv = job.maxv;
 
     for (int i = tid; i < OMS_MAX_BUCKETS * 4; i += nthr) (&s_cnt[0][0])[i] = 0;
     for (int i = tid; i < G * stride; i += nthr) Ps[i] = T(0);
-    for (int e = 0; e < tb.E; ++e) Rt[e * nthr] = T(0);
+    for (int e = 0; e < tb.E; ++e) Rt[e * rstride] = T(0);
     if (tid < 32) {
         const long long c0 = lo + tid, c1 = lo + G + tid;
         s_cur[tid] = tid < G && c0 < hi ? c0 : -1;
@@ -152,7 +157,7 @@ __device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJobT
                     if (j < d) {
                         const int e = eb + j;
                         addr[j] = gbase + tb.colz[e] + sp_wrap(t, tb.shift[e], z);
-                        const T Q = sp_sub(Ps[addr[j]], Rt[e * nthr]);
+                        const T Q = sp_sub(Ps[addr[j]], Rt[e * rstride]);
                         q[j] = Q;
                         T a = sp_sub(sp_abs(Q), beta);
                         a = a > T(0) ? a : T(0);
@@ -168,7 +173,7 @@ __device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJobT
                         const uint32_t sg = (rx ^ sp_signw(q[j])) & 0x80000000u;
                         const T rn = sp_flip(fj, sg);
                         Ps[addr[j]] = sp_add(q[j], rn);
-                        Rt[(eb + j) * nthr] = rn;
+                        Rt[(eb + j) * rstride] = rn;
                     }
                 }
             }
@@ -267,7 +272,7 @@ __device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJobT
         asm volatile("cp.async.commit_group;" ::: "memory");
         __syncthreads();
         if (active && (s_zero[par] & (1u << g)))
-            for (int e = 0; e < tb.E; ++e) Rt[e * nthr] = T(0);
+            for (int e = 0; e < tb.E; ++e) Rt[e * rstride] = T(0);
         if (!s_busy[par]) break;
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
