@@ -58,7 +58,8 @@ int setup_int(ldpc_ctx* x) {
     const int threads = ((G * c.z + 31) / 32) * 32;
     const size_t nstage_bytes = ((size_t)t.n * es + 15) & ~(size_t)15;
     const size_t base = ((((size_t)G * t.stride + 3) & ~(size_t)3) * 4) + (size_t)G * nstage_bytes;
-    const size_t r_smem = (size_t)t.E * threads * 4;
+    const size_t r_smem = (size_t)(t.E | 1) * threads * 4;   // shared: odd per-thread stride
+    const size_t r_glob = (size_t)t.E * threads * 4;          // global scratch: edge-major
     const bool rsmem = base + r_smem <= 160 * 1024;
     const size_t smem = base + (rsmem ? r_smem : 0);
     if (smem > (size_t)kSpMaxSmem) return fail(LDPC_ERR_UNSUPPORTED, "int%d decoder: %zu B of shared memory", bits, smem);
@@ -73,7 +74,7 @@ int setup_int(ldpc_ctx* x) {
     x->int_threads = threads;
     x->int_smem = (int)smem;
     x->int_ctas = per_sm * x->sms;
-    if (!rsmem) CUDA_TRY(cudaMalloc(&x->d_int_scratch, (size_t)x->int_ctas * r_smem));
+    if (!rsmem) CUDA_TRY(cudaMalloc(&x->d_int_scratch, (size_t)x->int_ctas * r_glob));
     // decode_row's offset and Max_row_simd in the element type (decode_functions.cpp:27-32, 59-62):
     // the float offset converts by truncation, the clamp is 1 - (CTYPE)max_row_metric for tiny values
     const double lim = bits == 16 ? 32767.0 : 2147483647.0;

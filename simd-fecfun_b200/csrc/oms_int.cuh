@@ -61,7 +61,7 @@ __device__ __forceinline__ int32_t int_abs(int32_t q) {
 }
 
 template <int W, int DMAX>
-__device__ __forceinline__ void int_layer(const SpTables& tb, int l, int32_t* Ps, int32_t* Rt, int nthr, int t,
+__device__ __forceinline__ void int_layer(const SpTables& tb, int l, int32_t* Ps, int32_t* Rt, int rstride, int t,
                                           int gbase, int beta, int maxv) {
     const int d = tb.rw[l], eb = tb.ebase[l], z = tb.z;
     int32_t q[DMAX];
@@ -73,7 +73,7 @@ __device__ __forceinline__ void int_layer(const SpTables& tb, int l, int32_t* Ps
         if (j < d) {
             const int e = eb + j;
             addr[j] = gbase + tb.colz[e] + sp_wrap(t, tb.shift[e], z);
-            const int32_t Q = int_sat<W>(Ps[addr[j]], Rt[e * nthr], true);
+            const int32_t Q = int_sat<W>(Ps[addr[j]], Rt[e * rstride], true);
             int32_t m = int_wrap<W>(int_abs<W>(Q) - beta);
             m = m > 0 ? m : 0;
             mn2 = min(mn2, max(mn1, m));
@@ -91,7 +91,7 @@ __device__ __forceinline__ void int_layer(const SpTables& tb, int l, int32_t* Ps
             const int32_t f = m == mn1 ? f2 : f1;
             const int32_t rn = ((rx ^ (uint32_t)q[j]) & 0x80000000u) ? -f : f;
             Ps[addr[j]] = int_sat<W>(q[j], rn, false);
-            Rt[(eb + j) * nthr] = rn;
+            Rt[(eb + j) * rstride] = rn;
         }
     }
 }
@@ -138,13 +138,18 @@ __global__ void __launch_bounds__(512) oms_int_kernel(const __grid_constant__ Sp
     const int nstage = ((n * (int)sizeof(TL) + 15) & ~15) / (int)sizeof(TL);
     int32_t* Rbase = RSMEM ? reinterpret_cast<int32_t*>(stage + G * nstage)
                            : job.r_scratch + (long long)blockIdx.x * tb.E * nthr;
-    int32_t* Rt = Rbase + tid;
+    // check messages: in shared memory each thread's E words are contiguous
+    // at an odd stride (E | 1: a warp's lanes fall in distinct banks), so edge
+    // e is the thread's base plus e; the global scratch keeps edge-major
+    // words (coalesced)
+    const int rstride = RSMEM ? 1 : nthr;
+    int32_t* Rt = RSMEM ? Rbase + tid * (tb.E | 1) : Rbase + tid;
     const TL* llr = reinterpret_cast<const TL*>(job.llr);
     const long long lo = job.ncw * blockIdx.x / gridDim.x, hi = job.ncw * (blockIdx.x + 1) / gridDim.x;
 
     for (int i = tid; i < OMS_MAX_BUCKETS * 4; i += nthr) (&s_cnt[0][0])[i] = 0;
     for (int i = tid; i < G * stride; i += nthr) Ps[i] = 0;
-    for (int e = 0; e < tb.E; ++e) Rt[e * nthr] = 0;
+    for (int e = 0; e < tb.E; ++e) Rt[e * rstride] = 0;
     if (tid < 32) {
         const long long c0 = lo + tid, c1 = lo + G + tid;
         s_cur[tid] = tid < G && c0 < hi ? c0 : -1;
@@ -170,7 +175,7 @@ __global__ void __launch_bounds__(512) oms_int_kernel(const __grid_constant__ Sp
 
     for (int par = 0;; par ^= 1) {
         for (int l = 0; l < tb.L; ++l) {
-            if (active) int_layer<W, DMAX>(tb, l, Ps, Rt, nthr, t, gbase, job.beta, job.maxv);
+            if (active) int_layer<W, DMAX>(tb, l, Ps, Rt, rstride, t, gbase, job.beta, job.maxv);
             __syncthreads();
         }
         if (tid == 0) {
@@ -274,7 +279,7 @@ __global__ void __launch_bounds__(512) oms_int_kernel(const __grid_constant__ Sp
         asm volatile("cp.async.commit_group;" ::: "memory");
         __syncthreads();
         if (active && (s_zero[par] & (1u << g)))
-            for (int e = 0; e < tb.E; ++e) Rt[e * nthr] = 0;
+            for (int e = 0; e < tb.E; ++e) Rt[e * rstride] = 0;
         if (!s_busy[par]) break;
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
