@@ -177,12 +177,18 @@ __device__ __forceinline__ void set_r(uint32_t (&R)[S::E_REG > 0 ? S::E_REG : 1]
     else k.Rs[(e - S::E_REG) * S::RS_STRIDE] = v;
 }
 
+// The posteriors the last layer writes are final for the iteration (no later
+// layer touches them), so the parity of this thread's last-layer row is the
+// XOR of the values it just wrote: the update keeps it in `plast` and the
+// syndrome neither recomputes those addresses nor reloads them.  Same
+// posteriors, same parity bit for bit.  (Keeping the final edges of earlier
+// layers as well costs a register each and spills.)
 // One layer of the layered update for this thread's check row t (all edges
 // of the row; the layer index is a template argument so every message
 // register index is a compile-time constant).
 template <class S, bool BETA0, int l>
 __device__ __forceinline__ void oms_layer(const OmsTables& tb, uint32_t* Ps, uint32_t (&R)[S::E_REG > 0 ? S::E_REG : 1], int t, int gbase,
-                                          const OmsConsts& k) {
+                                          const OmsConsts& k, uint32_t& plast) {
     constexpr int D = S::maxd(l);
     constexpr uint32_t SGN = 0x80008000u;
     uint32_t q[D];
@@ -226,6 +232,7 @@ __device__ __forceinline__ void oms_layer(const OmsTables& tb, uint32_t* Ps, uin
             const uint32_t Rn = M1 ^ (q[j] & SGN) ^ (eq & X);
             const uint32_t Pn = hmin2(hmax2(hadd2(q[j], Rn), H2_M128), H2_P127);
             Ps[addr[j]] = Pn;
+            if (l == S::L - 1) plast ^= Pn;
             set_r<S>(R, k, S::slot(l, j), Rn);
         }
     }
@@ -233,21 +240,24 @@ __device__ __forceinline__ void oms_layer(const OmsTables& tb, uint32_t* Ps, uin
 
 template <class S, bool BETA0, int l>
 __device__ __forceinline__ void oms_layer_sync(const OmsTables& tb, uint32_t* Ps, uint32_t (&R)[S::E_REG > 0 ? S::E_REG : 1], int t, int gbase,
-                                               bool active, const OmsConsts& k) {
-    if (active) oms_layer<S, BETA0, l>(tb, Ps, R, t, gbase, k);
+                                               bool active, const OmsConsts& k, uint32_t& plast) {
+    if (active) oms_layer<S, BETA0, l>(tb, Ps, R, t, gbase, k, plast);
     __syncthreads();
 }
 
 template <class S, bool BETA0, int... ls>
 __device__ __forceinline__ void oms_iteration(std::integer_sequence<int, ls...>, const OmsTables& tb, uint32_t* Ps,
-                                              uint32_t (&R)[S::E_REG > 0 ? S::E_REG : 1], int t, int gbase, bool active, const OmsConsts& k) {
-    (oms_layer_sync<S, BETA0, ls>(tb, Ps, R, t, gbase, active, k), ...);
+                                              uint32_t (&R)[S::E_REG > 0 ? S::E_REG : 1], int t, int gbase, bool active, const OmsConsts& k,
+                                              uint32_t& plast) {
+    (oms_layer_sync<S, BETA0, ls>(tb, Ps, R, t, gbase, active, k, plast), ...);
 }
 
-// OR over the layers of the XOR of the row's posteriors: sign bits 15/31 set
-// when a parity check of lane 0/1 fails.
+// XOR of the row's posteriors (the last layer's from the update): sign bits
+// 15/31 set when the parity check of lane 0/1 fails.
 template <class S, int l>
-__device__ __forceinline__ uint32_t oms_row_parity(const OmsTables& tb, const uint32_t* Ps, int t, int gbase) {
+__device__ __forceinline__ uint32_t oms_row_parity(const OmsTables& tb, const uint32_t* Ps, int t, int gbase,
+                                                   uint32_t plast) {
+    if (l == S::L - 1) return plast;
     uint32_t x = 0;
 #pragma unroll
     for (int j = 0; j < S::maxd(l); ++j) {
@@ -261,9 +271,9 @@ __device__ __forceinline__ uint32_t oms_row_parity(const OmsTables& tb, const ui
 // (the result, "some check of this codeword fails", is the same).
 template <class S, int l>
 __device__ __forceinline__ void oms_syndrome_step(const OmsTables& tb, const uint32_t* Ps, int t, int gbase,
-                                                  uint32_t* synd, uint32_t& seen, bool& stop) {
+                                                  uint32_t* synd, uint32_t& seen, bool& stop, uint32_t plast) {
     if (stop) return;
-    const uint32_t x = oms_row_parity<S, l>(tb, Ps, t, gbase) & 0x80008000u;
+    const uint32_t x = oms_row_parity<S, l>(tb, Ps, t, gbase, plast) & 0x80008000u;
     if (x & ~seen) {
         atomicOr(synd, x);
         seen |= x;
@@ -273,10 +283,11 @@ __device__ __forceinline__ void oms_syndrome_step(const OmsTables& tb, const uin
 
 template <class S, int... ls>
 __device__ __forceinline__ void oms_syndrome(std::integer_sequence<int, ls...>, const OmsTables& tb, const uint32_t* Ps,
-                                             int t, int gbase, uint32_t* synd) {
+                                             int t, int gbase, uint32_t* synd, uint32_t plast) {
     uint32_t seen = 0;
     bool stop = false;
-    (oms_syndrome_step<S, ls>(tb, Ps, t, gbase, synd, seen, stop), ...);
+    // last layer first: its parity needs no loads
+    (oms_syndrome_step<S, S::L - 1 - ls>(tb, Ps, t, gbase, synd, seen, stop, plast), ...);
 }
 
 // The same syndrome as a loop over the parameter-block tables: more
@@ -404,7 +415,8 @@ __global__ void __launch_bounds__(MAXT, MINB) oms_f16_kernel(const __grid_consta
         // gbase from loop-invariant code motion.
         int t_it = t, gbase_it = gbase;
         asm volatile("" : "+r"(t_it), "+r"(gbase_it));
-        oms_iteration<S, BETA0>(std::make_integer_sequence<int, S::L>(), tb, Ps, R, t_it, gbase_it, active, kc);
+        uint32_t plast = 0u;   // XOR of the posteriors the last layer writes
+        oms_iteration<S, BETA0>(std::make_integer_sequence<int, S::L>(), tb, Ps, R, t_it, gbase_it, active, kc, plast);
         // (the layer loop ends with a barrier) buffers of the other parity are free again
         if (tid < 16) {
             s_synd[par ^ 1][tid] = 0;
@@ -415,7 +427,7 @@ __global__ void __launch_bounds__(MAXT, MINB) oms_f16_kernel(const __grid_consta
         // ================= syndrome of every slot =================
         if (active) {
             if (job.synd_loop) oms_syndrome_loop<S>(tb, Ps, t_it, gbase_it, &s_synd[par][g]);
-            else oms_syndrome<S>(std::make_integer_sequence<int, S::L>(), tb, Ps, t_it, gbase_it, &s_synd[par][g]);
+            else oms_syndrome<S>(std::make_integer_sequence<int, S::L>(), tb, Ps, t_it, gbase_it, &s_synd[par][g], plast);
         }
         __syncthreads();
 
