@@ -148,6 +148,28 @@ def cpu_reference_rate(llr_sample, threads, per_thread_cw, reps):
     return reps * threads * per_thread_cw / wall, sum(iters), wall, sum(busy)
 
 
+def _ref_thread_inputs(rb, lib, code, per, snrs, seed, scale, max_abs):
+    """One host thread's sample for a reference build: `per` codewords split
+    evenly over every SNR point (one reference context per point), each made by
+    the reference's own pipeline (normdist2, gen_rand_databits, LDPCencode,
+    gen_metrics) from the thread's seeds.  Every thread decodes the same SNR
+    mix as the GPU step."""
+    import numpy as np
+    each = max(1, per // len(snrs))
+    out = []
+    for i, snr in enumerate(snrs):
+        with _quiet_stdout():
+            c = rb.RefCtx(lib, code, each)
+        seeds = (np.arange(64, dtype=np.uint64) + np.uint64(seed + 97 * i)) * np.uint64(0x9E3779B97F4A7C15) | np.uint64(1)
+        rb.ref_init_randstate(lib, seeds)
+        wgn = rb.ref_normdist2(lib, c.wgn_count())
+        c.gen_rand_databits()
+        c.encode()
+        c.gen_metrics(snr, wgn, scale, max_abs)
+        out.append(c)
+    return out
+
+
 def run_reference(args):
     """--impl reference: the reference's own CPU path on this box's host cores."""
     ws, rank, _ = _dist()
@@ -163,33 +185,26 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     lib = rb.RefLib("Vec64c_min")
     code = codes.make_code(CODE)
-    per = int(args.ref_sample)
-    # inputs through the reference's own pipeline (normdist2, gen_rand_databits,
-    # LDPCencode, gen_metrics), one SNR point per thread in rotation, untimed
-    ctxs = []
-    for k in range(threads):
-        with _quiet_stdout():
-            c = rb.RefCtx(lib, code, per)
-        seeds = (np.arange(64, dtype=np.uint64) + np.uint64(1000 + k)) * np.uint64(0x9E3779B97F4A7C15) | np.uint64(1)
-        rb.ref_init_randstate(lib, seeds)
-        wgn = rb.ref_normdist2(lib, c.wgn_count())
-        c.gen_rand_databits()
-        c.encode()
-        c.gen_metrics(SNRS[k % len(SNRS)], wgn, SCALE, MAX_ABS)
-        c.saved = c.metrics.copy()
-        ctxs.append(c)
+    # untimed inputs: every thread's sample split evenly over the five SNR points
+    ctxs = [_ref_thread_inputs(rb, lib, code, int(args.ref_sample), SNRS, 1000 + 1000 * k, SCALE, MAX_ABS)
+            for k in range(threads)]
+    for cs in ctxs:
+        for c in cs:
+            c.saved = c.metrics.copy()
+    per = sum(c.num_cw for c in ctxs[0])
     rates = []
     tot_iter = 0
     for step in range(args.warmup + args.steps):
-        for c in ctxs:
-            c.metrics[...] = c.saved
+        for cs in ctxs:
+            for c in cs:
+                c.metrics[...] = c.saved
         t0 = [0.0] * threads
         t1 = [0.0] * threads
         its = [0] * threads
 
         def work(k):
             t0[k] = time.perf_counter()
-            its[k] = ctxs[k].decode_set(MAX_ITER, MRM, BETA)
+            its[k] = sum(c.decode_set(MAX_ITER, MRM, BETA) for c in ctxs[k])
             t1[k] = time.perf_counter()
 
         th = [threading.Thread(target=work, args=(k,)) for k in range(threads)]
@@ -208,7 +223,7 @@ def run_reference(args):
         "data": "synthetic (the reference's own sfc64/xoshiro generators, gen_rand_databits, LDPCencode, gen_metrics)",
         "config": {"workload": WORKLOAD, "sample_per_step": threads * per,
                    "note": "each step decodes a bounded sample of the workload: %d codewords per host thread, "
-                           "SNR points assigned to threads in rotation" % per},
+                           "split evenly over the five SNR points" % per},
         "cpu_baseline": {"value": value, "unit": "codewords/s", "cores": threads, "kind": "reference",
                          "sample": "%d codewords per thread x %d threads per step" % (per, threads)},
         "e2e": {"value": value, "unit": "codewords/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -221,8 +236,8 @@ def run_reference(args):
 def ref_variant_rate(build, mrm, beta, scale, max_abs, threads, per, snrs, max_iter=10):
     """One reference build (oracle/_ref/libref_<build>.so) on host threads:
     inputs through the reference's own pipeline (normdist2,
-    gen_rand_databits, LDPCencode, gen_metrics) with the SNR points assigned
-    to threads in rotation, untimed; then LDPCdecode_set on every thread at
+    gen_rand_databits, LDPCencode, gen_metrics), every thread's sample split
+    evenly over the SNR points, untimed; then LDPCdecode_set on every thread at
     once, timed.  Returns (codewords/s, average iterations) or None when the
     build is absent."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -233,24 +248,15 @@ def ref_variant_rate(build, mrm, beta, scale, max_abs, threads, per, snrs, max_i
         return None
     lib = rb.RefLib(build)
     code = codes.make_code(CODE, elem_size=abs(lib.elem_bw))
-    ctxs = []
-    for k in range(threads):
-        with _quiet_stdout():
-            c = rb.RefCtx(lib, code, per)
-        seeds = (np.arange(64, dtype=np.uint64) + np.uint64(2000 + k)) * np.uint64(0x9E3779B97F4A7C15) | np.uint64(1)
-        rb.ref_init_randstate(lib, seeds)
-        wgn = rb.ref_normdist2(lib, c.wgn_count())
-        c.gen_rand_databits()
-        c.encode()
-        c.gen_metrics(snrs[k % len(snrs)], wgn, scale, max_abs)
-        ctxs.append(c)
+    ctxs = [_ref_thread_inputs(rb, lib, code, per, snrs, 2000 + 1000 * k, scale, max_abs) for k in range(threads)]
+    per = sum(c.num_cw for c in ctxs[0])
     t0 = [0.0] * threads
     t1 = [0.0] * threads
     its = [0] * threads
 
     def work(k):
         t0[k] = time.perf_counter()
-        its[k] = ctxs[k].decode_set(max_iter, mrm, beta)
+        its[k] = sum(c.decode_set(max_iter, mrm, beta) for c in ctxs[k])
         t1[k] = time.perf_counter()
 
     th = [threading.Thread(target=work, args=(k,)) for k in range(threads)]
@@ -430,7 +436,7 @@ def main():
 
     import numpy as np
     import torch
-    from ldpc_b200 import capi, codes
+    from ldpc_b200 import capi, codes, sharding
 
     ws, rank, local = _dist()
     torch.cuda.set_device(local)
@@ -454,7 +460,9 @@ def main():
     llr = torch.empty((nsnr, nps, N), dtype=torch.int8, device="cuda")
     data = torch.empty((nps, HW), dtype=torch.int32, device="cuda")
     unc = torch.zeros(nsnr, dtype=torch.int64, device="cuda")
-    ctx.generate(seed=2024, cw_offset=rank * nps, snr_db=SNRS, n_per_snr=nps, llr_i8=llr, data_bits=data,
+    # this rank's share of the global codeword range (disjoint Philox counters)
+    cw_start, _ = sharding.weak_shard(nps, rank, ws)
+    ctx.generate(seed=2024, cw_offset=cw_start, snr_db=SNRS, n_per_snr=nps, llr_i8=llr, data_bits=data,
                  uncoded=unc, stream=sptr)
     hard = torch.empty((total, HW), dtype=torch.int32, device="cuda")
     iters = torch.empty(total, dtype=torch.uint8, device="cuda")
@@ -488,14 +496,7 @@ def main():
     clocks = _clock_summary(clk)
     elapsed_ms = t_start.elapsed_time(t_stop)
     launch_ms = [a.elapsed_time(b) for a, b in ev]
-    if dist:
-        t = torch.tensor([elapsed_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
-        c_all = counters.clone()
-        dist.all_reduce(c_all)
-    else:
-        c_all = counters
+    c_all, elapsed_ms = sharding.finish_run(counters, elapsed_ms)
     cnt = c_all.cpu().numpy()
     value = ws * total * args.steps / (elapsed_ms * 1e-3)
     ms_per_step = elapsed_ms / args.steps

@@ -384,10 +384,15 @@ int ldpc_count_errors(ldpc_ctx *ctx, const uint32_t *hard, size_t n, const uint3
  * Arguments and outputs are those of ldpc_decode_f32 (dev pointers, async on
  * `stream`), on the CURRENT device; cfg's llr_scale / max_abs_llr are unused.
  *
+ * Shared memory and codes accepted are the context path's: any code that
+ * ldpc_ctx_create takes for a float variant (5G NR base graph 1 at Z=384 and
+ * 802.3ca run without the LLR staging buffer, as there).
+ *
  * The first call on each device does the setup: symbol lookup and kernel
- * attributes.  Make it before any stream capture, from one thread.  Two calls
- * whose kernels may overlap on the same device race on the shared array:
- * order them (one stream, or events). */
+ * attributes.  Make it before any stream capture.  Later calls take no lock.
+ * After cudaDeviceReset on a device that has used it, do not call it again in
+ * that process.  Two calls whose kernels may overlap on the same device race
+ * on the shared array: order them (one stream, or events). */
 int ldpc_decode_f32_noalloc(const ldpc_code *code, const ldpc_cfg *cfg, const float *llr, size_t n,
                             float *post_out, uint32_t *hard_out, uint8_t *iters_out, void *stream);
 

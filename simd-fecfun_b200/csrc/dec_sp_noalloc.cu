@@ -27,9 +27,17 @@
 //     and corrupt each other's messages.  Order them on one stream, or with
 //     events.
 //   - The first call on each device looks up the array's address and sets the
-//     kernels' shared-memory limit.  Make it before any stream capture, and
-//     from one host thread.
+//     kernels' shared-memory limit.  Make it before any stream capture.  Later
+//     calls take no lock: they read a per-device ready flag.
+//   - The cached address belongs to the device's current context: after
+//     cudaDeviceReset on a device that has used this entry point, the entry
+//     point must not be called again in that process.
+//   - Shared memory: posteriors and LLR staging of G codewords per CTA, G as
+//     the context path picks it, within the same 220 KB limit; a code whose
+//     single codeword does not fit with its staging buffer runs without it
+//     (5G NR base graph 1 at Z=384, 802.3ca), as the context path does.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 
@@ -41,7 +49,10 @@ namespace {
 constexpr size_t kScratchBytes = 32u << 20;     // 32 MiB per device
 constexpr int kMaxDevices = 64;
 constexpr int kThreads = 512;                   // __launch_bounds__ of the kernels below
-constexpr int kMaxSmem = 200 * 1024;
+// The kernels are the context path's instances (sp_f32_kernel<D, P, false, 512>),
+// and a kernel's shared-memory limit is a property of the function: both
+// paths set it to the same maximum, so neither lowers it under the other.
+constexpr int kMaxSmem = ldpc::kSpMaxSmem;
 
 __device__ __align__(256) float g_sp_scratch[kScratchBytes / sizeof(float)];
 
@@ -55,7 +66,7 @@ const NoallocKernel kKernels[] = {SPN(8, true), SPN(8, false), SPN(16, true), SP
 #undef SPN
 
 struct DeviceState {
-    bool ready = false;
+    std::atomic<bool> ready{false};
     float* scratch = nullptr;
     int sms = 0;
 };
@@ -63,11 +74,16 @@ DeviceState g_dev[kMaxDevices];
 std::mutex g_setup_mu;
 
 // Once per device, with that device current: the scratch address, the SM
-// count, and the dynamic shared-memory limit of every kernel variant.
+// count, and the dynamic shared-memory limit of every kernel variant.  After
+// that a call reads the ready flag (acquire) and takes no lock.
 int device_setup(int dev, DeviceState** out) {
-    std::lock_guard<std::mutex> lock(g_setup_mu);
     DeviceState& d = g_dev[dev];
-    if (!d.ready) {
+    if (d.ready.load(std::memory_order_acquire)) {
+        *out = &d;
+        return LDPC_OK;
+    }
+    std::lock_guard<std::mutex> lock(g_setup_mu);
+    if (!d.ready.load(std::memory_order_relaxed)) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_sp_scratch);
         if (e != cudaSuccess)
@@ -78,7 +94,7 @@ int device_setup(int dev, DeviceState** out) {
         for (const NoallocKernel& k : kKernels)
             CUDA_TRY(cudaFuncSetAttribute((const void*)k.k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
         d.scratch = (float*)p;
-        d.ready = true;
+        d.ready.store(true, std::memory_order_release);
     }
     *out = &d;
     return LDPC_OK;
@@ -111,34 +127,22 @@ extern "C" int ldpc_decode_f32_noalloc(const ldpc_code* code, const ldpc_cfg* cf
     if (int rc = device_setup(dev, &ds)) return rc;
     if (n == 0) return LDPC_OK;
 
-    // tables by value in the kernel parameters: the layout of the context
-    // path's setup, with the messages always in the scratch array
+    // tables by value in the kernel parameters, codewords per CTA and the
+    // staging rule of the context path (setup_sp); the messages always live
+    // in the scratch array
     ldpc::SpTables t;
-    memset(&t, 0, sizeof(t));
-    t.z = c.z;
-    t.mcol = c.mcol;
-    t.n = c.z * c.mcol;
-    t.L = c.mrow;
-    t.kbits = c.z * (c.mcol - c.mrow);
-    t.hard_words = (t.kbits + 31) / 32;
-    t.E = (int)c.row_cols.size();
-    int e0 = 0;
-    for (int l = 0; l < c.mrow; ++l) {
-        t.rw[l] = (int16_t)c.row_weights[l];
-        t.ebase[l] = (int16_t)e0;
-        e0 += c.row_weights[l];
-    }
-    for (int e = 0; e < t.E; ++e) {
-        t.colz[e] = c.row_cols[e] * c.z;
-        t.shift[e] = (int16_t)c.row_shifts[e];
-    }
     int G = std::max(1, std::min(32, 128 / c.z));
     while (G > 1 && ((G * c.z + 31) / 32) * 32 > kThreads) --G;
-    t.G = G;
-    t.stride = t.n + ((((32 + G - 1) / G) - t.n) % 32 + 32) % 32;
+    const int nstage = (c.z * c.mcol + 3) & ~3;
+    auto base_bytes = [&](int g, bool stage) {
+        ldpc::fill_sp_tables(c, g, &t);
+        return ((((size_t)g * t.stride + 3) & ~(size_t)3) + (stage ? (size_t)g * nstage : 0)) * sizeof(float);
+    };
+    while (G > 1 && base_bytes(G, true) > (size_t)kMaxSmem) --G;
+    const bool nostage = base_bytes(G, true) > (size_t)kMaxSmem;
+    const size_t smem = base_bytes(G, !nostage);   // leaves t filled for G
+    t.nostage = nostage ? 1 : 0;
     const int threads = ((G * c.z + 31) / 32) * 32;
-    const int nstage = (t.n + 3) & ~3;
-    const size_t smem = ((((size_t)G * t.stride + 3) & ~(size_t)3) + (size_t)G * nstage) * 4;
     if (smem > (size_t)kMaxSmem) return fail(LDPC_ERR_UNSUPPORTED, "float decoder: %zu B of shared memory", smem);
     const size_t per_cta = (size_t)t.E * threads * sizeof(float);
     if (per_cta > kScratchBytes)

@@ -5,7 +5,7 @@ min_find_wrap.pl does: ``min_find.pl <d> prod``) for every row weight and
 writes ``min_find_trees.json``: for d <= 32 the full statement list
 (node masks in hex), for 33..53 a SHA-256 of the statement list.
 
-    python tests/golden/make_tree_golden.py /root/reference
+    python tests/golden/make_tree_golden.py <reference checkout>
 """
 import hashlib
 import json
