@@ -190,12 +190,12 @@ int orc_decode_f32(const orc_code *c, const orc_trees *tr, int mode, const float
                         Q[j] = P[v[j]] - R[(size_t)(e0 + j) * z + t];
                         float a = fabsf(Q[j]) - beta;
                         a = a > 0.0f ? a : 0.0f;
-                        x[j] = mode ? lm_tanh(a * 0.5f) : a;
+                        x[j] = mode == 1 ? lm_tanh(a * 0.5f) : mode == 2 ? (float)tanh((double)(a * 0.5f)) : a;
                         rx ^= fbits(Q[j]);
                     }
-                    run_tree_f32(tr->prog + 4 * tr->off[d], tr->len[d], d, mode, x, maxv, node, f);
+                    run_tree_f32(tr->prog + 4 * tr->off[d], tr->len[d], d, mode != 0, x, maxv, node, f);
                     for (int j = 0; j < d; ++j) {
-                        float fj = mode ? 2.0f * lm_atanh(f[j]) : f[j];
+                        float fj = mode == 1 ? 2.0f * lm_atanh(f[j]) : mode == 2 ? 2.0f * (float)atanh((double)f[j]) : f[j];
                         uint32_t s = rx ^ fbits(Q[j]);
                         float rn = (s & 0x80000000u) ? bitsf(fbits(fj) ^ 0x80000000u) : fj;
                         P[v[j]] = Q[j] + rn;
@@ -282,12 +282,12 @@ int orc_decode_f64(const orc_code *c, const orc_trees *tr, int mode, const doubl
                         Q[j] = P[v[j]] - R[(size_t)(e0 + j) * z + t];
                         double a = fabs(Q[j]) - b;
                         a = a > 0.0 ? a : 0.0;
-                        x[j] = mode ? lmd_tanh(a * 0.5) : a;
+                        x[j] = mode == 1 ? lmd_tanh(a * 0.5) : mode == 2 ? tanh(a * 0.5) : a;
                         rx ^= dbits(Q[j]);
                     }
-                    run_tree_f64(tr->prog + 4 * tr->off[d], tr->len[d], d, mode, x, maxv, node, f);
+                    run_tree_f64(tr->prog + 4 * tr->off[d], tr->len[d], d, mode != 0, x, maxv, node, f);
                     for (int j = 0; j < d; ++j) {
-                        double fj = mode ? 2.0 * lmd_atanh(f[j]) : f[j];
+                        double fj = mode == 1 ? 2.0 * lmd_atanh(f[j]) : mode == 2 ? 2.0 * atanh(f[j]) : f[j];
                         uint64_t s = (rx ^ dbits(Q[j])) & 0x8000000000000000ULL;
                         double rn = bitsd(dbits(fj) ^ s);
                         P[v[j]] = Q[j] + rn;
@@ -425,4 +425,39 @@ int64_t orc_llr_array(const uint8_t *bits, const float *noise, size_t total, int
         if (llr_i8) llr_i8[e] = (int8_t)(int16_t)li;
     }
     return errs;
+}
+
+/* The shared tanh / atanh over arrays, so that tests can measure their error
+ * against the C library's long-double functions. */
+void orc_lm_tanh_array(const float *x, float *y, size_t n) { for (size_t i = 0; i < n; ++i) y[i] = lm_tanh(x[i]); }
+void orc_lm_atanh_array(const float *x, float *y, size_t n) { for (size_t i = 0; i < n; ++i) y[i] = lm_atanh(x[i]); }
+void orc_lmd_tanh_array(const double *x, double *y, size_t n) { for (size_t i = 0; i < n; ++i) y[i] = lmd_tanh(x[i]); }
+void orc_lmd_atanh_array(const double *x, double *y, size_t n) { for (size_t i = 0; i < n; ++i) y[i] = lmd_atanh(x[i]); }
+
+/* Largest error, in units in the last place of float, of the shared float
+ * tanh (kind 0) or atanh (kind 1) against the C library's long-double
+ * tanhl / atanhl, over the non-negative floats whose bit patterns run from
+ * lo_bits to hi_bits (inclusive) in steps of `stride`.  The ulp of a true
+ * value v is 2^(floor(log2 |v|) - 23).  Returns the input with the largest
+ * error in *argmax. */
+double orc_ulp_scan_f32(int kind, uint32_t lo_bits, uint32_t hi_bits, uint32_t stride, float *argmax) {
+    double worst = 0.0;
+    float wx = 0.0f;
+    for (uint64_t b = lo_bits; b <= hi_bits; b += stride) {
+        const float x = bitsf((uint32_t)b);
+        const float y = kind ? lm_atanh(x) : lm_tanh(x);
+        const long double v = kind ? atanhl((long double)x) : tanhl((long double)x);
+        double u = 0.0;
+        if (v != 0.0L) {
+            int e;
+            frexpl(v, &e);                               /* |v| in [2^(e-1), 2^e) */
+            const long double ulp = ldexpl(1.0L, e - 1 - 23);
+            u = (double)(fabsl((long double)y - v) / ulp);
+        } else if (y != 0.0f) {
+            u = INFINITY;
+        }
+        if (u > worst) { worst = u; wx = x; }
+    }
+    if (argmax) *argmax = wx;
+    return worst;
 }

@@ -52,15 +52,30 @@ int orc_decode_int8_tree(const orc_code *c, const orc_trees *t, const int8_t *ll
                          unsigned max_iter, float max_row_metric, float beta, int8_t *post_out,
                          uint32_t *iters_out);
 
-/* mode 0 = min-sum tree, 1 = sum-product (tanh/atanh) tree */
+/* mode 0 = min-sum tree, 1 = sum-product (tanh/atanh) tree with the shared
+ * ldpc_math.h functions (what the GPU runs), 2 = sum-product with the C
+ * library's tanh/atanh evaluated in double and rounded to float: an
+ * independent transcendental, for reporting how far the shared one moves the
+ * decode (not bit parity) */
 int orc_decode_f32(const orc_code *c, const orc_trees *t, int mode, const float *llr, size_t n_cw,
                    unsigned max_iter, float max_row_metric, float beta, float *post_out,
                    uint32_t *iters_out);
 
-/* the same decoder in double precision (the reference's Vec8d builds) */
+/* the same decoder in double precision (the reference's Vec8d builds);
+ * mode 2 = the C library's double tanh/atanh */
 int orc_decode_f64(const orc_code *c, const orc_trees *t, int mode, const double *llr, size_t n_cw,
                    unsigned max_iter, float max_row_metric, float beta, double *post_out,
                    uint32_t *iters_out);
+
+/* the shared tanh / atanh (ldpc_math.h) elementwise over arrays */
+void orc_lm_tanh_array(const float *x, float *y, size_t n);
+void orc_lm_atanh_array(const float *x, float *y, size_t n);
+void orc_lmd_tanh_array(const double *x, double *y, size_t n);
+void orc_lmd_atanh_array(const double *x, double *y, size_t n);
+
+/* largest ulp error of the shared float tanh (kind 0) / atanh (kind 1)
+ * against long-double tanhl / atanhl over float bit patterns lo..hi, step stride */
+double orc_ulp_scan_f32(int kind, uint32_t lo_bits, uint32_t hi_bits, uint32_t stride, float *argmax);
 
 /* sigma and LLR factor exactly as gen_metrics.cpp:26-30 computes them */
 void orc_sigma(float snr, float llr_scale, float *sigma, float *sigma_factor);

@@ -209,6 +209,21 @@ class Oracle:
                                        keep[2].ctypes.data_as(p), 53), keep)
         return self._trees[0]
 
+    def shared_math(self, name, x):
+        """The shared tanh / atanh (ldpc_math.h) elementwise: name in
+        {"tanh", "atanh"}; float32 input runs the float functions, float64 the
+        double ones."""
+        x = np.ascontiguousarray(x)
+        if x.dtype == np.float32:
+            fn = {"tanh": self.lib.orc_lm_tanh_array, "atanh": self.lib.orc_lm_atanh_array}[name]
+        elif x.dtype == np.float64:
+            fn = {"tanh": self.lib.orc_lmd_tanh_array, "atanh": self.lib.orc_lmd_atanh_array}[name]
+        else:
+            raise TypeError("float32 or float64 input")
+        y = np.empty_like(x)
+        fn(x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p), C.c_size_t(x.size))
+        return y
+
     def decode_int8(self, code, llr, max_iter=10, max_row_metric=31.0, beta=1.0, use_tree=False, beta_layers=None,
                     beta_table=None):
         """int8 layered offset min-sum; ``beta_layers`` (one int8 offset per
