@@ -391,6 +391,8 @@ def run_workload(args):
         out = run_variants(args, clk)
     elif args.workload == "sim":
         out = run_sim(args)
+    elif args.workload == "offset-search":
+        out = workloads.offset_search(n_search=args.search_n, n_valid=args.search_valid_n)
     else:
         out = workloads.learned_run(train_steps=max(args.steps, 2), batch=args.learned_batch,
                                     weights=args.learned_weights)
@@ -418,7 +420,7 @@ def main():
     ap.add_argument("--variant-ref-sample", type=int, default=4000,
                     help="int8 codewords per host thread for the reference builds (--workload variants)")
     ap.add_argument("--workload", default="11ad",
-                    choices=["11ad", "nr-mix", "hetero-mix", "learned", "sp-sweep", "variants", "sim"],
+                    choices=["11ad", "nr-mix", "hetero-mix", "learned", "sp-sweep", "variants", "sim", "offset-search"],
                     help="11ad: the headline run; others: the batched 5G NR mix, the 18-code 802.11 mix "
                          "(plain vs learned offsets), learned-offset training, the float sum-product Z sweep, "
                          "every decoder variant on the headline point, the process-level drop-in against the "
@@ -426,7 +428,10 @@ def main():
     ap.add_argument("--llr-budget-gb", type=float, default=40.0, help="nr-mix: LLR bytes the codeword counts are scaled to")
     ap.add_argument("--no-autotune", action="store_true", help="nr-mix: default launch shape")
     ap.add_argument("--learned-batch", type=int, default=65536)
-    ap.add_argument("--learned-weights", default="uniform", choices=["uniform", "early"])
+    ap.add_argument("--search-n", type=int, default=4_000_000, help="offset-search: codewords of the search set")
+    ap.add_argument("--search-valid-n", type=int, default=20_000_000,
+                    help="offset-search: fresh codewords that validate the best table")
+    ap.add_argument("--learned-weights", default="uniform", choices=["uniform", "early", "steep"])
     ap.add_argument("--sp-cw", type=int, default=1 << 20, help="sp-sweep: codewords per Z")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -464,6 +469,22 @@ def main():
     cw_start, _ = sharding.weak_shard(nps, rank, ws)
     ctx.generate(seed=2024, cw_offset=cw_start, snr_db=SNRS, n_per_snr=nps, llr_i8=llr, data_bits=data,
                  uncoded=unc, stream=sptr)
+    # the generator itself (untimed for the headline): the same call again, timed by events;
+    # algorithmic bytes = the int8 LLRs of every SNR point + the packed data bits
+    gen_ms = []
+    for _ in range(3):
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        ctx.generate(seed=2024, cw_offset=cw_start, snr_db=SNRS, n_per_snr=nps, llr_i8=llr, data_bits=data,
+                     uncoded=unc, stream=sptr)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        gen_ms.append(g0.elapsed_time(g1))
+    gen_bytes = total * N + nps * HW * 4
+    generation = {"kernel": "gen_kernel", "ms": statistics.median(gen_ms), "bytes": gen_bytes,
+                  "achieved_gbs": gen_bytes / (statistics.median(gen_ms) * 1e-3) / 1e9,
+                  "what": "%d codewords: data bits, QC encoding, one AWGN draw per bit, int8 LLRs at %d SNR points"
+                          % (nps, nsnr)}
     hard = torch.empty((total, HW), dtype=torch.int32, device="cuda")
     iters = torch.empty(total, dtype=torch.uint8, device="cuda")
     counters = torch.zeros((nsnr, 4), dtype=torch.int64, device="cuda")
@@ -544,6 +565,7 @@ def main():
         roofline["hbm"]["peak_gbs"] = hbm_peak
         roofline["hbm"]["frac"] = roofline["hbm"]["achieved_gbs"] / hbm_peak
         roofline["hbm"]["peak_source"] = "MEASURED_PEAKS.json (measured)"
+        generation["frac_of_hbm"] = generation["achieved_gbs"] / hbm_peak
     except (OSError, KeyError, ValueError):
         pass
 
@@ -612,7 +634,7 @@ def main():
                    "l2": "inputs larger than L2 (%.2f GB of LLRs per step per GPU)" % (total * N / 1e9),
                    "info_gbps": value * 336 / 1e9},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps, "clocks": clocks,
-        "quality": quality,
+        "quality": quality, "generation": generation,
     }
     if rank == 0:
         print(json.dumps(line))

@@ -404,6 +404,12 @@ int ldpc_decode_f32_noalloc(const ldpc_code *code, const ldpc_cfg *cfg, const fl
  * in the reference (which times with RDTSC only, LDPCtop.cpp:107-114). */
 int ldpc_probe_int32_peak(int device, double *ops_per_s);
 
+/* Sustained FP32 fused multiply-add rate and MUFU (ex2.approx) rate of
+ * `device` (instructions per second, one per thread per op), from chains of
+ * independent operations: the denominators of the float decoders' roofline.
+ * No counterpart in the reference. */
+int ldpc_probe_fp32_peak(int device, double *fma_per_s, double *mufu_per_s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,6 +20,30 @@ void sigma_of(float snr, float llr_scale, float* sigma, float* sf) {
     *sf = 2 * llr_scale / (s * s);
 }
 
+// Tile shape of gen_kernel: the per-thread encoder for Z <= 64 without filler
+// bits, 128 codewords per tile (halved until the tile fits 96 KB); else the
+// warp encoder, 32 codewords per tile (halved until it fits 100 KB).
+size_t gen_tile_shape(const GenTables& t, GenTile* tile) {
+    const size_t nw = t.n / 32 + 3, dwp = t.kbits / 32 + 3;
+    tile->thread_enc = (t.z <= 64 && !t.any_filler) ? 1 : 0;
+    size_t smem = 0;
+    if (tile->thread_enc) {
+        int T = 128;
+        auto bytes = [&](int T_) { return (size_t)T_ * (8 * (size_t)t.mcol + 4 * (dwp + nw)); };
+        while (T > 1 && bytes(T) > 96 * 1024) T /= 2;
+        tile->T = T;
+        smem = bytes(T);
+    } else {
+        int T = 32;
+        const size_t warp_bytes = 4 * (size_t)(GEN_THREADS / 32) * gen_warp_words(t.kbits, t.mcol, t.z, t.n);
+        auto bytes = [&](int T_) { return 4 * nw * T_ + warp_bytes; };
+        while (T > 1 && bytes(T) > 100 * 1024) T /= 2;
+        tile->T = T;
+        smem = bytes(T);
+    }
+    return smem;
+}
+
 int gen_grid(ldpc_ctx* x, long long n, int* smem) {
     const GenTables& t = x->gent;
     *smem = gen_warp_words(t.kbits, t.mcol, t.z, t.n) * 4 * 8;
@@ -62,6 +86,9 @@ int setup_gen(ldpc_ctx* x) {
     int smem = 0;
     gen_grid(x, 1, &smem);
     if (smem > 200 * 1024) return fail(LDPC_ERR_UNSUPPORTED, "generator needs %d B of shared memory", smem);
+    GenTile tile;
+    const size_t gsmem = gen_tile_shape(t, &tile);
+    if (gsmem > 200 * 1024) return fail(LDPC_ERR_UNSUPPORTED, "generator tile needs %zu B of shared memory", gsmem);
     CUDA_TRY(allow_dynamic_smem((const void*)gen_kernel, 200 * 1024));
     CUDA_TRY(allow_dynamic_smem((const void*)encode_kernel, 200 * 1024));
     return LDPC_OK;
@@ -101,9 +128,16 @@ int launch_gen(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* snr_
     job.llr_f32 = llr_f32;
     job.data_bits = data_bits;
     job.uncoded = uncoded;
-    int smem = 0;
-    const int grid = gen_grid(x, (long long)n_per_snr, &smem);
-    gen_kernel<<<grid, 256, smem, s>>>(x->gent, job);
+    GenTile tile;
+    const size_t smem = gen_tile_shape(x->gent, &tile);
+    // int8 output alone, whole 4-element blocks, a clamp the rounding trick covers
+    tile.fast = (job.llr_i8 && !job.llr_f32 && !job.llr_i16 && !job.llr_i32 && !job.llr_f64 && (x->gent.n & 3) == 0 &&
+                 std::fabs(job.max_abs) < 2097152.0f && n_snr <= (size_t)GEN_FAST_SNR) ? 1 : 0;
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)gen_kernel, GEN_THREADS, smem));
+    const long long tiles = ((long long)n_per_snr + tile.T - 1) / tile.T;
+    const int grid = (int)std::max<long long>(1, std::min<long long>(tiles, (long long)x->sms * std::max(per_sm, 1)));
+    gen_kernel<<<grid, GEN_THREADS, smem, s>>>(x->gent, job, tile);
     CUDA_TRY(cudaGetLastError());
     return LDPC_OK;
 }

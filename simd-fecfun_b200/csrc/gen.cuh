@@ -171,49 +171,230 @@ __device__ void draw_data_warp(const GenTables& tb, uint64_t seed, uint64_t cw, 
     }
 }
 
-__global__ void __launch_bounds__(256) gen_kernel(const __grid_constant__ GenTables tb, const __grid_constant__ GenJob job) {
-    extern __shared__ uint32_t sm[];
-    __shared__ unsigned long long s_unc[GEN_MAX_SNR];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int wpw = gen_warp_words(tb.kbits, tb.mcol, tb.z, tb.n);
-    uint32_t* data = sm + warp * wpw;
-    uint32_t* cols = data + (tb.kbits / 32 + 2);
-    uint32_t* cwbits = cols + tb.mcol * ((tb.z + 31) / 32 + 1);
-    for (int i = threadIdx.x; i < GEN_MAX_SNR; i += blockDim.x) s_unc[i] = 0;
-    __syncthreads();
-    unsigned long long unc[GEN_MAX_SNR];
-#pragma unroll
-    for (int s = 0; s < GEN_MAX_SNR; ++s) unc[s] = 0;
+// ---- fused generation over tiles of codewords ----
+//
+// A CTA takes tiles of T consecutive codewords.  Phase A encodes the tile
+// into shared memory as bit streams, bits[w * T + c] = word w of codeword c;
+// phase B runs the noise and the LLRs of the tile's n/4 four-bit blocks per
+// codeword with every thread busy: item f = (c, b) gives one Philox block,
+// two Box-Muller pairs and four LLRs per SNR point, stored as one 4-byte word
+// per SNR row, so a warp writes 128 contiguous bytes.
+//
+// Phase A for Z <= 64 and no filler bits (gen_encode_thread): one thread per
+// codeword, each column one 64-bit word in shared memory (cols[c * T + t]),
+// a parity column the XOR of columns rotated by their shifts.  Otherwise one
+// warp per codeword (encode_warp).
 
-    const long long nwarps_total = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long i = (long long)blockIdx.x * (blockDim.x >> 5) + warp; i < job.n_per_snr; i += nwarps_total) {
-        const uint64_t cw = job.cw_offset + (uint64_t)i;
-        draw_data_warp(tb, job.seed, cw, data, lane);
-        if (job.data_bits)
-            for (int w = lane; w < tb.hard_words; w += 32) job.data_bits[i * tb.hard_words + w] = data[w];
-        encode_warp(tb, data, cols, cwbits, lane);
-        // noise + LLRs, 4 bits per lane per Philox block
-        for (int b = lane; 4 * b < tb.n; b += 32) {
+constexpr int GEN_THREADS = 256;
+
+// x rotated so that bit i of the result is bit (i + s) mod z of x (z <= 64, s < z)
+__device__ __forceinline__ uint64_t rotr_z(uint64_t x, int s, int z, uint64_t mask) {
+    return s == 0 ? x : (((x >> s) | (x << (z - s))) & mask);
+}
+
+// Per-thread encoder: data words dat[w * T + t] (kbits bits, LSB first) ->
+// codeword bit stream bits[w * T + t] (nw words).  cols is 8-byte aligned.
+__device__ void gen_encode_thread(const GenTables& tb, const uint32_t* dat, uint64_t* cols, uint32_t* bits, int T,
+                                  int t, int nw) {
+    const int z = tb.z, kc = tb.mcol - tb.mrow;
+    const uint64_t mask = z == 64 ? ~0ull : ((1ull << z) - 1ull);
+    for (int c = 0; c < kc; ++c) {
+        const int p = c * z, w = p >> 5, sh = p & 31;
+        const uint32_t a = dat[w * T + t], b = dat[(w + 1) * T + t], d = dat[(w + 2) * T + t];
+        const uint64_t v = (uint64_t)__funnelshift_r(a, b, sh) | ((uint64_t)__funnelshift_r(b, d, sh) << 32);
+        cols[c * T + t] = v & mask;
+    }
+    for (int r = 0; r < tb.n_par; ++r) {
+        const int first = tb.par_first[r], cnt = tb.par_cnt[r];
+        uint64_t acc = 0;
+        for (int q = 0; q < cnt; ++q) acc ^= rotr_z(cols[tb.term_col[first + q] * T + t], tb.term_shift[first + q] % z, z, mask);
+        cols[tb.par_col[r] * T + t] = acc;
+    }
+    for (int w = 0; w < nw; ++w) bits[w * T + t] = 0u;
+    for (int c = 0; c < tb.mcol; ++c) {
+        const uint64_t v = cols[c * T + t];
+        const int p = c * z, w = p >> 5, sh = p & 31;
+        const uint32_t lo = (uint32_t)v, hi = (uint32_t)(v >> 32);
+        bits[w * T + t] |= lo << sh;
+        bits[(w + 1) * T + t] |= (sh ? (lo >> (32 - sh)) : 0u) | (hi << sh);
+        if (sh) bits[(w + 2) * T + t] |= hi >> (32 - sh);
+    }
+}
+
+// Box-Muller pair with the hardware approximations of log2, sqrt and
+// sin/cos (absolute errors ~2^-21; the noise is checked statistically).
+// u1 = (w_r + 1/2) 2^-32, refined by a second word down to 2^-65 when
+// w_r < 256 (tail to ~9.5 sigma); angle = pi * (int)w_a * 2^-31 in [-pi, pi).
+__device__ __forceinline__ float2 box_muller_fast(uint32_t w_r, uint32_t w_a, uint64_t seed, uint64_t cw,
+                                                  uint32_t block, int which) {
+    float u1;
+    if (w_r < 256u) {
+        const uint4 x = philox_at(seed, cw, block, 2u);
+        const uint32_t w2 = which ? x.z : x.x;
+        u1 = fmaf((float)w_r, 0x1p-32f, fmaf((float)w2, 0x1p-64f, 0x1p-65f));
+    } else {
+        u1 = fmaf((float)w_r, 0x1p-32f, 0x1p-33f);
+    }
+    float r;
+    const float e = fmaxf(-1.38629436f * __log2f(u1), 0.0f);   // -2 ln u1 = -2 ln2 log2 u1
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(e));
+    float sn, cs;
+    __sincosf((float)(int)w_a * 1.46291808e-9f, &sn, &cs);    // pi / 2^31
+    return make_float2(r * cs, r * sn);
+}
+
+// Sign bit of each of four floats replicated over one byte: byte q = 0xff
+// when x_q is negative.
+__device__ __forceinline__ uint32_t sign_bytes4(float x0, float x1, float x2, float x3) {
+    uint32_t a, b, d;
+    asm("prmt.b32 %0, %1, %2, 0x00FB;" : "=r"(a) : "r"(__float_as_uint(x0)), "r"(__float_as_uint(x1)));
+    asm("prmt.b32 %0, %1, %2, 0x00FB;" : "=r"(b) : "r"(__float_as_uint(x2)), "r"(__float_as_uint(x3)));
+    asm("prmt.b32 %0, %1, %2, 0x5410;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+
+// Layout of a tile in dynamic shared memory, as the host sizes it:
+//   thread encoder (Z <= 64): cols [mcol][T] uint64, dat [dwp][T], bits [nw][T]
+//   warp encoder:             bits [nw][T], then per warp gen_warp_words scratch
+// with nw = n/32 + 3 and dwp = kbits/32 + 3 (one spare zero word past each
+// stream for the encoder's three-word reads and writes).
+struct GenTile {
+    int T;              // codewords per tile
+    int thread_enc;     // 1: gen_encode_thread, 0: encode_warp
+    int fast;           // 1: int8 output only, n % 4 == 0, |max_abs| < 2^21, at most GEN_FAST_SNR points
+};
+constexpr int GEN_FAST_SNR = 8;
+
+// gen_metrics for four elements at every SNR point, the int8 output only:
+// rx = fma(noise, sigma, orig), l = rx * sf, clamp to [-max_abs, max_abs]
+// (these three steps as llr_element does them), then round-half-even by
+// adding 1.5 * 2^23 (exact for |l| < 2^21) and keeping the low byte, which
+// is (int8)(int16)roundi(l).  Punctured elements give 0, filler elements
+// roundi(max_abs).  The uncoded error of an element is the sign of rx
+// against the sent sign; counts go to unc[s] (8 x the count: one bit per
+// byte of a sign mask, divided out at the end).
+__device__ __forceinline__ void llr4_i8_fast(const GenJob& job, long long i, long long row_stride, int idx0,
+                                             const float (&nz)[4], uint32_t bits4, uint32_t pmask, uint32_t fmask,
+                                             uint32_t fbytes, unsigned (&unc)[GEN_FAST_SNR]) {
+    float o[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) o[q] = ((bits4 >> q) & 1u) ? -1.0f : 1.0f;
+    const uint32_t osign = sign_bytes4(o[0], o[1], o[2], o[3]);
+    const float ma = job.max_abs;
+#pragma unroll
+    for (int s = 0; s < GEN_FAST_SNR; ++s) {
+        if (s < job.n_snr) {
+            const float sg = job.sigma[s], sf = job.sigma_factor[s];
+            float rx[4];
+            uint32_t t[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                rx[q] = fmaf(nz[q], sg, o[q]);
+                float l = __fmul_rn(rx[q], sf);
+                l = ma < l ? ma : l;
+                l = -ma > l ? -ma : l;
+                t[q] = __float_as_uint(__fadd_rn(l, 12582912.0f));
+            }
+            uint32_t packed = __byte_perm(__byte_perm(t[0], t[1], 0x0040), __byte_perm(t[2], t[3], 0x0040), 0x5410);
+            packed = (packed & ~(pmask | fmask)) | (fbytes & fmask);
+            *reinterpret_cast<uint32_t*>(job.llr_i8 + ((long long)s * job.n_per_snr + i) * row_stride + idx0) = packed;
+            unc[s] += __popc(sign_bytes4(rx[0], rx[1], rx[2], rx[3]) ^ osign);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(GEN_THREADS) gen_kernel(const __grid_constant__ GenTables tb,
+                                                          const __grid_constant__ GenJob job, const GenTile tile) {
+    extern __shared__ __align__(16) uint32_t sm[];
+    __shared__ unsigned long long s_unc[GEN_MAX_SNR];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int T = tile.T;
+    const int nw = tb.n / 32 + 3, dwp = tb.kbits / 32 + 3, nb = (tb.n + 3) / 4;
+    uint64_t* cols = reinterpret_cast<uint64_t*>(sm);
+    uint32_t* dat = sm + 2 * tb.mcol * T;
+    uint32_t* bits = tile.thread_enc ? dat + dwp * T : sm;
+    uint32_t* wscr = sm + nw * T + warp * gen_warp_words(tb.kbits, tb.mcol, tb.z, tb.n);
+    for (int i = tid; i < GEN_MAX_SNR; i += blockDim.x) s_unc[i] = 0;
+    unsigned unc_f[GEN_FAST_SNR];
+#pragma unroll
+    for (int s = 0; s < GEN_FAST_SNR; ++s) unc_f[s] = 0;
+    const long long ntiles = (job.n_per_snr + T - 1) / T;
+    for (long long tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+        const long long i0 = tl * T;
+        const int tc = (int)min((long long)T, job.n_per_snr - i0);
+        __syncthreads();   // the previous tile's bits are consumed
+        // ---- phase A: data bits and encoding of the tile's codewords ----
+        if (tile.thread_enc) {
+            if (tid < tc) {
+                const uint64_t cw = job.cw_offset + (uint64_t)(i0 + tid);
+                for (int b = 0; 4 * b < dwp; ++b) {
+                    const uint4 x = philox_at(job.seed, cw, (uint32_t)b, 0u);
+                    const uint32_t v[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int w = 4 * b + q;
+                        if (w < dwp) {
+                            uint32_t m = v[q];
+                            const int lo = w * 32;
+                            if (lo + 32 > tb.kbits) m &= (lo >= tb.kbits) ? 0u : ((1u << (tb.kbits - lo)) - 1u);
+                            dat[w * T + tid] = m;
+                            if (job.data_bits && w < tb.hard_words) job.data_bits[(i0 + tid) * tb.hard_words + w] = m;
+                        }
+                    }
+                }
+                gen_encode_thread(tb, dat, cols, bits, T, tid, nw);
+            }
+        } else {
+            uint32_t* data = wscr;
+            uint32_t* wcols = data + (tb.kbits / 32 + 2);
+            uint32_t* cwbits = wcols + tb.mcol * ((tb.z + 31) / 32 + 1);
+            for (int c = warp; c < tc; c += GEN_THREADS / 32) {
+                const uint64_t cw = job.cw_offset + (uint64_t)(i0 + c);
+                draw_data_warp(tb, job.seed, cw, data, lane);
+                if (job.data_bits)
+                    for (int w = lane; w < tb.hard_words; w += 32) job.data_bits[(i0 + c) * tb.hard_words + w] = data[w];
+                encode_warp(tb, data, wcols, cwbits, lane);
+                for (int w = lane; w < tb.n / 32 + 2; w += 32) bits[w * T + c] = cwbits[w];
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        // ---- phase B: noise and LLRs, item f = codeword c, block b of 4 bits ----
+        const long long row_stride = tb.n;
+        for (int f = tid; f < tc * nb; f += GEN_THREADS) {
+            const int c = f / nb, b = f - c * nb;
+            const long long i = i0 + c;
+            const uint64_t cw = job.cw_offset + (uint64_t)i;
             const uint4 x = philox_at(job.seed, cw, (uint32_t)b, 1u);
-            const float2 g0 = box_muller(x.x, x.y, job.seed, cw, (uint32_t)b, 0);
-            const float2 g1 = box_muller(x.z, x.w, job.seed, cw, (uint32_t)b, 1);
+            const float2 g0 = box_muller_fast(x.x, x.y, job.seed, cw, (uint32_t)b, 0);
+            const float2 g1 = box_muller_fast(x.z, x.w, job.seed, cw, (uint32_t)b, 1);
             const float nz[4] = {g0.x, g0.y, g1.x, g1.y};
             const int idx0 = 4 * b;
-            const uint32_t bits4 = (stream_bits32(cwbits, idx0)) & 0xfu;
+            const uint32_t bits4 = (bits[(idx0 >> 5) * T + c] >> (idx0 & 31)) & 0xfu;
+            if (tile.fast) {
+                uint32_t pmask = 0u, fmask = 0u;
+                if (tb.any_punct) pmask = *reinterpret_cast<const uint32_t*>(tb.punct + idx0) * 0xffu;
+                if (tb.any_filler) fmask = *reinterpret_cast<const uint32_t*>(tb.filler + idx0) * 0xffu;
+                const uint32_t fbyte = (uint32_t)__float2int_rn(job.max_abs) & 0xffu;
+                llr4_i8_fast(job, i, row_stride, idx0, nz, bits4, pmask, fmask, fbyte * 0x01010101u, unc_f);
+                continue;
+            }
             for (int s = 0; s < job.n_snr; ++s) {
                 float l[4];
                 uint32_t packed = 0;
+                unsigned e = 0;
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const int idx = idx0 + q;
                     if (idx < tb.n) {
                         const int pn = tb.any_punct ? tb.punct[idx] : 0;
                         const int fl = tb.any_filler ? tb.filler[idx] : 0;
-                        unc[s] += llr_element((bits4 >> q) & 1u, nz[q], job.sigma[s], job.sigma_factor[s], job.max_abs,
-                                              pn, fl, &l[q]);
+                        e += llr_element((bits4 >> q) & 1u, nz[q], job.sigma[s], job.sigma_factor[s], job.max_abs, pn,
+                                         fl, &l[q]);
                         packed |= (uint32_t)(uint8_t)llr_to_i8(l[q]) << (8 * q);
                     }
                 }
+                if (e && job.uncoded) atomicAdd(&s_unc[s], (unsigned long long)e);
                 const long long row = (long long)s * job.n_per_snr + i;
                 if (job.llr_i8) {
                     int8_t* dst = job.llr_i8 + row * tb.n + idx0;
@@ -243,17 +424,22 @@ __global__ void __launch_bounds__(256) gen_kernel(const __grid_constant__ GenTab
                 }
             }
         }
-        __syncwarp();
     }
     if (job.uncoded) {
-        for (int s = 0; s < job.n_snr; ++s) {
-            unsigned long long v = unc[s];
+        if (tile.fast) {
+            // each error counted 8 times (one per bit of a 0xff byte)
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0 && v) atomicAdd(&s_unc[s], v);
+            for (int s = 0; s < GEN_FAST_SNR; ++s) {
+                if (s < job.n_snr) {
+                    unsigned long long v = unc_f[s] >> 3;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                    if (lane == 0 && v) atomicAdd(&s_unc[s], v);
+                }
+            }
         }
         __syncthreads();
-        for (int s = threadIdx.x; s < job.n_snr; s += blockDim.x)
+        for (int s = tid; s < job.n_snr; s += blockDim.x)
             if (s_unc[s]) atomicAdd(job.uncoded + s, s_unc[s]);
     }
 }

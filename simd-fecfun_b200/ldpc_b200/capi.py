@@ -97,6 +97,7 @@ _PROTOS = {
     "ldpc_count_errors": (C.c_int, [_vp, _vp, _sz, _vp, _sz, _vp, _vp]),
     "ldpc_decode_count": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _sz, _sz, _vp, C.c_int, _vp]),
     "ldpc_probe_int32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+    "ldpc_probe_fp32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "ldpc_decode_f32_noalloc": (C.c_int, [_vp, C.POINTER(Cfg), _vp, _sz, _vp, _vp, _vp, _vp]),
     "ldpc_batch_create": (C.c_int, [C.POINTER(_vp), C.POINTER(Cfg), C.c_int, C.c_int, C.POINTER(_vp)]),
     "ldpc_batch_set_offsets": (C.c_int, [_vp, C.c_int, _vp]),
@@ -143,6 +144,13 @@ def probe_int32_peak(device: int = 0) -> float:
     v = C.c_double()
     check(lib.ldpc_probe_int32_peak(device, C.byref(v)))
     return v.value
+
+
+def probe_fp32_peak(device: int = 0):
+    """(FP32 fused multiply-adds per second, MUFU ops per second) of the device."""
+    f, m = C.c_double(), C.c_double()
+    check(lib.ldpc_probe_fp32_peak(device, C.byref(f), C.byref(m)))
+    return f.value, m.value
 
 
 def _ptr(x) -> Optional[int]:

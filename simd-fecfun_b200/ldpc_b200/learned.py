@@ -173,13 +173,19 @@ def _rank_world(group=None):
 
 def train(ctx, code, iters: int = 10, batch: int = 65536, steps: int = 100, ebn0=(1.0, 2.5), lr: float = 0.01,
           init: float = 0.5, seed: int = 1, n_snr: int = 16, loss_w: Optional[Sequence[float]] = None, log=None,
-          group=None):
+          group=None, quant_step: Optional[float] = None):
     """Adam on beta [iters][mrow] (initialised to ``init``); every step draws
     a fresh batch at Eb/N0 points spread uniformly over ``ebn0``.  With a
     process group, ``batch`` is per rank: rank r draws codewords
     [(step * world + r) * batch, ...) of the generator's stream, the ranks
     share the Eb/N0 draw (same ``seed``) and average their gradients, so
-    their offsets stay identical."""
+    their offsets stay identical.
+
+    ``quant_step``: quantisation-aware training for offsets that will be
+    deployed on a grid (0.5 for the int8 decoder at LLR scale 2, whose
+    offsets are integers in its own units): the decoder runs with beta
+    rounded to the grid, the gradient passes the rounding unchanged
+    (straight-through), and the returned offsets are on the grid."""
     rank, world = _rank_world(group)
     rate = code.k / (code.n - code.punc_cnt_bits - code.fill_cnt)
     beta = torch.full((iters, code.mrow), init, dtype=torch.float32, device="cuda", requires_grad=True)
@@ -191,7 +197,8 @@ def train(ctx, code, iters: int = 10, batch: int = 65536, steps: int = 100, ebn0
         eb = rng.uniform(ebn0[0], ebn0[1], n_snr)
         llr, bits = draw(ctx, code, batch, [snr_from_ebn0(e, rate) for e in eb], seed, (step * world + rank) * batch)
         opt.zero_grad()
-        loss = LearnedOMSLoss.apply(beta, llr, bits, w, ctx)
+        b_used = beta if quant_step is None else beta + (torch.round(beta / quant_step) * quant_step - beta).detach()
+        loss = LearnedOMSLoss.apply(b_used, llr, bits, w, ctx)
         loss.backward()
         average_gradients([beta], group)
         opt.step()
@@ -200,6 +207,8 @@ def train(ctx, code, iters: int = 10, batch: int = 65536, steps: int = 100, ebn0
         history.append(float(loss))
         if log:
             log(step, float(loss))
+    if quant_step is not None:
+        return (torch.round(beta.detach() / quant_step) * quant_step), history
     return beta.detach(), history
 
 

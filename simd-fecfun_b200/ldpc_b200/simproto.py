@@ -43,3 +43,23 @@ def fold_seeds(seeds):
         x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & m
         k = x ^ (x >> 31)
     return k
+
+
+def run_hash(blob_bytes: bytes, variant: int) -> int:
+    """The parameter hash ldpc_sim writes in its state file header (FNV-1a
+    over the blob with the outer count zeroed, and the seeds zeroed unless
+    use_given_rand_state is 1, then the decoder variant)."""
+    b = bytearray(blob_bytes)
+    b[0:4] = b"\0\0\0\0"
+    if struct.unpack_from("<i", b, 20)[0] != 1:
+        b[52:52 + 512] = bytes(512)
+    m = (1 << 64) - 1
+    h = 0xCBF29CE484222325
+    for v in b:
+        h = ((h ^ v) * 0x100000001B3) & m
+    return ((h ^ (variant & 0xFFFFFFFF)) * 0x100000001B3) & m
+
+
+def state_text(blob_bytes: bytes, variant: int, key: int, lines) -> str:
+    """A state file as ldpc_sim writes it (LDPC_SIM_STATE)."""
+    return "ldpc_sim state v1 %016x %016x\n" % (run_hash(blob_bytes, variant), key) + "".join(l + "\n" for l in lines)

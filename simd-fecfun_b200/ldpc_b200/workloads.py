@@ -77,6 +77,34 @@ def _quality(specs, meta, names, objs, steps) -> List[Dict]:
     return out
 
 
+# Roofline work units.
+# int8 offset min-sum: 10 int8 lane-ops per edge and iteration (Q sub, abs,
+# offset, clamp at 0, min1/min2 update (2), sign XOR, select, sign apply, P
+# add), four lanes per 32-bit op: 2.5 packed int32 ops per edge-iteration,
+# against the probed int32 issue rate.
+INT8_OPS_PER_EDGE = 2.5
+# float sum-product: FP32 operations per edge-iteration of the update as
+# written (ldpc_math.h along its usual branches, a division counted once):
+# tanh 23 (-2x, Cody-Waite e^y with a degree-8 Horner polynomial, -e/(2+e)),
+# atanh 27 (2m/(1-m), log1p by exponent split, a degree-6 series in s^2 and
+# the first-order correction), the rest of the edge 8 (P - R, |Q| - beta,
+# max 0, x 0.5, ~2.3 tree products, 2 x atanh, Q + R'), against the probed
+# FP32 fused multiply-add rate.
+SP_FP32_OPS_PER_EDGE = 58.0
+
+
+def _edge_iters_per_step(specs, quality, objs, steps) -> float:
+    """Edge updates per timed step: codewords x average iterations x edges,
+    summed over the jobs (quality holds the counters of ``steps`` steps)."""
+    return sum(q["codewords"] * q["avg_iter"] * objs[sp["code"]].edges for sp, q in zip(specs, quality)) / steps
+
+
+def _roofline(work_per_step: float, ms: float, peak: float, unit: str, definition: str, peak_source: str) -> Dict:
+    achieved = work_per_step / (ms * 1e-3)
+    return {"bound": unit.split()[0], "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "T%s/s" % unit,
+            "frac": achieved / peak, "definition": definition, "peak_source": peak_source}
+
+
 def _time_plan(plan, specs, steps, warmup, graph=True):
     s = torch.cuda.current_stream()
     for _ in range(warmup):
@@ -115,6 +143,11 @@ def nr_mix(steps: int = 3, warmup: int = 1, seed: int = 7, llr_budget: float = 4
     total = sum(counts)
     info_bits = sum(m * c.k for m, c in zip(counts, objs))
     avg_ms = sum(ms) / len(ms)
+    roofline = _roofline(_edge_iters_per_step(specs, quality, objs, steps) * INT8_OPS_PER_EDGE, avg_ms,
+                         capi.probe_int32_peak(torch.cuda.current_device()), "int32 ops",
+                         "sum over jobs of codewords x iterations x edges x 2.5 packed int32 ops (10 int8 lane-ops "
+                         "per edge-iteration, 4 lanes per 32-bit op), per step, over the step's graph time",
+                         "own microbenchmark of 32-bit lop3/iadd chains (ldpc_probe_int32_peak)")
     # the same jobs, one code at a time through the per-code entry point
     s = torch.cuda.current_stream()
     ctxs = [capi.Context(h, max_iter=20) for h in handles]
@@ -148,6 +181,7 @@ def nr_mix(steps: int = 3, warmup: int = 1, seed: int = 7, llr_budget: float = 4
         "info_gbps": info_bits / (avg_ms * 1e-3) / 1e9,
         "per_code_sequential": {"value": total / (seq_ms * 1e-3), "unit": "codewords/s",
                                 "note": "same jobs, one ldpc_decode_count launch per job"},
+        "roofline": roofline,
         "gpu_launches": steps * plan.kernels,
         "quality": quality,
     }
@@ -203,7 +237,7 @@ def hetero_mix(steps: int = 3, warmup: int = 1, total: int = 10_000_000, seed: i
                             llr_scale=1.0, max_abs_llr=1e9)
         eb = snr[ci] - 10.0 * math.log10(_rate(c))
         beta, _ = learned.train(fctx, c, iters=10, batch=8192, steps=train_steps, ebn0=(eb - 0.25, eb + 0.25), lr=0.02,
-                                init=0.5, seed=seed + ci, n_snr=4)
+                                init=0.5, seed=seed + ci, n_snr=4, quant_step=0.5)
         b8 = np.clip(np.rint(2.0 * beta.cpu().numpy()), 0, 127).astype(np.float32)   # [iters][layers]
         batch.set_offset_table(ci, b8)
         offsets.append(b8.astype(int).tolist())
@@ -229,8 +263,9 @@ def hetero_mix(steps: int = 3, warmup: int = 1, total: int = 10_000_000, seed: i
         "learned": {"value": total / (avg_learned * 1e-3), "unit": "codewords/s", "avg_iter": it_l,
                     "offsets_int8": dict(zip(names, offsets)), "training_s": round(train_s, 1),
                     "training": "float offset min-sum, 10 iterations, %d Adam steps of 8192 codewords at the "
-                                "calibrated SNR +-0.25 dB; offsets x2 (int8 LLR scale), rounded, deployed as an "
-                                "int8 [iteration][layer] table" % train_steps},
+                                "calibrated SNR +-0.25 dB, quantisation-aware (offsets rounded to multiples of 0.5, "
+                                "straight-through gradient); offsets x2 (int8 LLR scale) deployed as an int8 "
+                                "[iteration][layer] table" % train_steps},
         "plain_avg_iter": it_p,
         "gpu_launches": steps * plan.kernels,
         "quality_plain": q_plain, "quality_learned": q_learned,
@@ -239,9 +274,9 @@ def hetero_mix(steps: int = 3, warmup: int = 1, total: int = 10_000_000, seed: i
 
 def learned_run(train_steps: int = 30, batch: int = 65536, eval_n: int = 200_000, seed: int = 3,
                 weights: str = "uniform") -> Dict:
-    """``weights``: "uniform" (every iteration's BCE counts once) or "early"
+    """``weights``: "uniform" (every iteration's BCE counts once), "early"
     (iteration it weighted 1/(it+1), rewarding codewords that are right
-    sooner)."""
+    sooner) or "steep" (weight 2^-it: the first iterations dominate)."""
     code = codes.make_code("16e 1/2", z_over=96)
     h = capi.Code.from_tables(code)
     ctx = capi.Context(h, variant=capi.LDPC_F32_OMS, max_iter=10, max_row_metric=31.0, beta=0.5, llr_scale=1.0,
@@ -251,7 +286,8 @@ def learned_run(train_steps: int = 30, batch: int = 65536, eval_n: int = 200_000
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    lw = [1.0 / (i + 1) for i in range(10)] if weights == "early" else None
+    lw = ([1.0 / (i + 1) for i in range(10)] if weights == "early" else
+          [0.5 ** i for i in range(10)] if weights == "steep" else None)
     beta, hist = learned.train(ctx, code, iters=10, batch=batch, steps=train_steps, ebn0=(1.0, 2.5), lr=0.01,
                                init=0.5, seed=seed, loss_w=lw)
     e1.record()
@@ -344,6 +380,13 @@ def sp_sweep(cw_per_z: int = 1 << 20, ebn0=(0.5, 1.0, 1.5, 2.0), seed: int = 5, 
     total = sum(sp["n"] for sp in specs)
     info_bits = sum(sp["n"] * objs[sp["code"]].k for sp in specs)
     avg_ms = sum(ms) / len(ms)
+    fma_peak, mufu_peak = capi.probe_fp32_peak(torch.cuda.current_device())
+    roofline = _roofline(_edge_iters_per_step(specs, quality, objs, steps) * SP_FP32_OPS_PER_EDGE, avg_ms, fma_peak,
+                         "fp32 ops",
+                         "sum over jobs of codewords x iterations x edges x 58 FP32 operations per edge-iteration "
+                         "(tanh 23, atanh 27, the rest of the update 8), per step, over the step's graph time",
+                         "own microbenchmark of FP32 fma chains (ldpc_probe_fp32_peak)")
+    roofline["mufu_peak"] = mufu_peak / 1e12
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(s)
     for sp in specs:
@@ -371,6 +414,7 @@ def sp_sweep(cw_per_z: int = 1 << 20, ebn0=(0.5, 1.0, 1.5, 2.0), seed: int = 5, 
         "info_gbps": info_bits / (avg_ms * 1e-3) / 1e9,
         "per_launch_sequential": {"value": total / (seq_ms * 1e-3), "unit": "codewords/s",
                                   "note": "same jobs, one ldpc_decode_count launch per (Z, Eb/N0)"},
+        "roofline": roofline,
         "gpu_launches": steps * plan.kernels,
         "quality": quality,
     }
@@ -415,3 +459,181 @@ def variants(n_per_snr: int = 200_000, snrs=(-1.0, -0.75, -0.5, -0.25, 0.0), see
                          "ber": x["bit_errors"] / (x["codewords"] * code.k)} for x in st],
         })
     return out
+
+
+def _cwer_ci(err: int, n: int):
+    """95 % Wilson interval of a codeword error rate."""
+    if n == 0:
+        return (0.0, 1.0)
+    p, z = err / n, 1.96
+    den = 1 + z * z / n
+    c = (p + z * z / (2 * n)) / den
+    h = z * math.sqrt(p * (1 - p) / n + z * z / (4 * n * n)) / den
+    return (max(0.0, c - h), min(1.0, c + h))
+
+
+def _coord_search(run, S, base, values, sweeps, limit, it0):
+    """Coordinate descent over an offset table: minimise the average
+    iterations ``run(table, S)[0]`` subject to codeword errors
+    ``run(table, S)[1] <= limit``; first whole rows (one offset per
+    iteration), then single entries.  Returns (table, avg_iter, trace)."""
+    best, best_it = base.copy(), it0
+    trace = []
+    rows, cols = best.shape
+
+    def consider(tab):
+        nonlocal best, best_it
+        it, e = run(tab, S)
+        if e <= limit and it < best_it - 1e-9:
+            best, best_it = tab.copy(), it
+
+    for _ in range(sweeps):
+        for i in range(rows):
+            for v in values:
+                if np.all(best[i] == v):
+                    continue
+                tab = best.copy()
+                tab[i, :] = v
+                consider(tab)
+        trace.append(round(best_it, 5))
+    for _ in range(sweeps):
+        for i in range(rows):
+            for l in range(cols):
+                for v in values:
+                    if v == best[i, l]:
+                        continue
+                    tab = best.copy()
+                    tab[i, l] = v
+                    consider(tab)
+        trace.append(round(best_it, 5))
+    return best, best_it, trace
+
+
+def _search_point(run, S, V, base, values, sweeps, label, n_search, n_valid):
+    it0, e0 = run(None, S)
+    limit = e0 + 2.0 * math.sqrt(max(e0, 1))
+    best, best_it, trace = _coord_search(run, S, base, values, sweeps, limit, it0)
+    itp, ep = run(None, V)
+    itb, eb = run(best, V)
+    return {
+        "point": label,
+        "search": {"codewords": n_search, "plain_avg_iter": it0, "plain_cw_errors": e0, "best_avg_iter": best_it,
+                   "feasible_cw_errors_max": limit, "trace_avg_iter": trace},
+        "validation": {"codewords": n_valid,
+                       "plain": {"avg_iter": itp, "cw_errors": ep, "cwer": ep / n_valid, "cwer_ci95": _cwer_ci(ep, n_valid)},
+                       "best": {"avg_iter": itb, "cw_errors": eb, "cwer": eb / n_valid, "cwer_ci95": _cwer_ci(eb, n_valid)},
+                       "iter_reduction": 1.0 - itb / itp},
+        "best_table": best.tolist(),
+    }
+
+
+def offset_search(snr_db=(0.0, -0.5), n_search: int = 4_000_000, n_valid: int = 20_000_000,
+                  values=(0, 1, 2, 3, 4), sweeps: int = 2, max_iter: int = 10, seed: int = 21,
+                  f_ebn0=(3.0103, 2.0), f_search: int = 400_000, f_valid: int = 2_000_000,
+                  f_values=(0.0, 0.25, 0.5, 0.75, 1.0, 1.5)) -> Dict:
+    """Empirical ceiling of the iteration saving that offsets alone can buy:
+    a coordinate search over offset tables beta[iteration][layer], run with
+    the GPU decoders themselves.
+
+    int8 (the headline code, 802.11ad 1/2, Es/N0 ``snr_db``): integer offsets
+    in ``values`` (the reference truncates its one offset to an integer for
+    the int8 build, decode_functions.cpp:59-62), the plain decoder being
+    beta = 1 everywhere (the Perl driver's default).  Float offset min-sum
+    (802.16e 1/2 Z=96, the learned decoder's code, Eb/N0 ``f_ebn0``; 3.01 dB
+    is the reference's SNR of 0 dB at rate 1/2): offsets in ``f_values``,
+    plain beta = 0.5.
+
+    Per point, LLRs of a search set and of a fresh validation set are drawn
+    once and stay in HBM.  The plain table's codeword errors e0 on the
+    search set set the constraint: a table is feasible when its errors are
+    at most e0 + 2 sqrt(e0).  The search minimises the average iterations over
+    feasible tables (whole rows first, then single entries, ``sweeps`` passes
+    each); the best table and the plain one are then decoded on the
+    validation set and reported with 95 % intervals."""
+    t_start = time.time()
+    n_evals = 0
+    s = torch.cuda.current_stream().cuda_stream
+    cnt = torch.zeros((1, 4), dtype=torch.int64, device="cuda")
+    points = []
+
+    # ---- int8, 802.11ad rate 1/2 ----
+    code = codes.make_code("11ad 1/2")
+    ctx = capi.Context(capi.Code.from_tables(code), max_iter=max_iter, max_row_metric=31.0, beta=1.0, llr_scale=2.0,
+                       max_abs_llr=24.0)
+    N, HW = code.n, ctx.info.hard_words
+
+    def make8(n, snr, off):
+        llr = torch.empty((1, n, N), dtype=torch.int8, device="cuda")
+        data = torch.empty((n, HW), dtype=torch.int32, device="cuda")
+        ctx.generate(seed, off, [snr], n, llr_i8=llr, data_bits=data, stream=s)
+        return llr, data, n
+
+    def run8(table, st):
+        nonlocal n_evals
+        llr, data, n = st
+        ctx.set_offset_table(None if table is None else np.asarray(table, np.float32))
+        cnt.zero_()
+        ctx.decode_count(llr, n, data_bits=data, ref_period=n, bucket_size=n, counters=cnt, n_buckets=1, stream=s)
+        c = cnt.cpu().numpy()[0]
+        n_evals += 1
+        return float(c[1]) / n, int(c[3])
+
+    for snr in snr_db:
+        S, V = make8(n_search, snr, 0), make8(n_valid, snr, 1 << 36)
+        r = _search_point(run8, S, V, np.ones((max_iter, code.mrow), np.float32), values, sweeps,
+                          "802.11ad 1/2 int8, Es/N0 %.2f dB" % snr, n_search, n_valid)
+        r["best_table"] = np.asarray(r["best_table"]).astype(int).tolist()
+        points.append(r)
+        del S, V
+    ctx.set_offset_table(None)
+
+    # ---- float offset min-sum, 802.16e rate 1/2 Z=96 (the learned decoder's code) ----
+    fcode = codes.make_code("16e 1/2", z_over=96)
+    fctx = capi.Context(capi.Code.from_tables(fcode), variant=capi.LDPC_F32_OMS, max_iter=max_iter,
+                        max_row_metric=31.0, beta=0.5, llr_scale=1.0, max_abs_llr=1e9)
+    kb, fhw = fctx.info.kbits, fctx.info.hard_words
+    pw = (2 ** torch.arange(32, dtype=torch.int64, device="cuda"))
+
+    def makef(n, snr, off):
+        llr, bits = learned.draw(fctx, fcode, n, [snr], seed, off)
+        ref = torch.zeros((n, fhw * 32), dtype=torch.int64, device="cuda")
+        ref[:, :kb] = bits[:, :kb].to(torch.int64)
+        ref = (ref.view(n, fhw, 32) * pw).sum(dim=2).to(torch.uint32).view(torch.int32)
+        del bits
+        return llr, ref, n
+
+    hard = torch.empty((f_valid, fhw), dtype=torch.int32, device="cuda")
+    its = torch.empty(f_valid, dtype=torch.uint8, device="cuda")
+
+    def runf(table, st):
+        nonlocal n_evals
+        llr, ref, n = st
+        beta = torch.as_tensor(np.full((max_iter, fcode.mrow), 0.5, np.float32) if table is None else
+                               np.asarray(table, np.float32), device="cuda").contiguous()
+        capi.check(capi.lib.ldpc_learned_decode(fctx.h, llr.data_ptr(), n, max_iter, beta.data_ptr(), None,
+                                                hard.data_ptr(), its.data_ptr(), s or None))
+        e = int((hard[:n] != ref).any(dim=1).sum())
+        n_evals += 1
+        return float(its[:n].sum()) / n, e
+
+    for eb in f_ebn0:
+        snr = learned.snr_from_ebn0(eb, 0.5)
+        S, V = makef(f_search, snr, 0), makef(f_valid, snr, 1 << 36)
+        r = _search_point(runf, S, V, np.full((max_iter, fcode.mrow), 0.5, np.float32), f_values, sweeps,
+                          "802.16e 1/2 Z=96 float, Eb/N0 %.2f dB (Es/N0 %.2f dB)" % (eb, snr), f_search, f_valid)
+        points.append(r)
+        del S, V
+    return {
+        "metric": "average iterations at matched codeword error rate, offset min-sum with searched offset tables "
+                  "beta[iteration][layer] vs the plain offset",
+        "value": max(p["validation"]["iter_reduction"] for p in points), "unit": "fraction of iterations saved",
+        "n_gpus": 1, "higher_is_better": True, "vs_baseline": None, "dtype": "int8 and f32",
+        "data": "synthetic: Philox data bits, QC encoding, AWGN from the fused generator, resident in HBM",
+        "config": {"workload": "int8: 802.11ad 1/2, LLR scale 2, max|LLR| 24, Max 31, offsets %s, plain 1; float: "
+                               "802.16e 1/2 Z=96, Max 31, offsets %s, plain 0.5; %d max iterations; coordinate search, "
+                               "%d sweeps per stage (rows, then entries); feasible = codeword errors on the search set "
+                               "<= e0 + 2 sqrt(e0)" % (list(values), list(f_values), max_iter, sweeps),
+                   "evaluations": n_evals, "search_s": round(time.time() - t_start, 1)},
+        "points": points,
+        "gpu_launches": n_evals,
+    }

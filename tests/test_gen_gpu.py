@@ -171,3 +171,40 @@ def test_integer_llrs_match_reference_gen_metrics(capi, variant, bits, scale, ma
     # the fused generator quantises the same way: its int16/int32 LLRs decode in simulate
     st = ctx.simulate(seed=5, cw_offset=0, snr_db=[1.0], n_per_snr=5000)[0]
     assert st["codewords"] == 5000 and st["iterations"] >= 5000
+
+
+@pytest.mark.parametrize("name,n", [("11ad 1/2", 3000), ("16e 1/2", 2000), ("11n 5/6 z81", 1500),
+                                    ("5GNR_n3136_k576", 1000), ("5GNR_n1000_k500", 1000), ("5GNR_n25344_k8448", 120),
+                                    ("5GNR_n2048_k704 bg1 z32", 1000)])
+def test_generate_int8_path_matches_float_path(capi, name, n):
+    """The generator's int8-only path (four LLRs rounded and packed per word,
+    uncoded errors from sign masks) against its general path on the same
+    seed: identical data bits and uncoded counts, and int8 LLRs equal to the
+    float LLRs rounded half-even.  Covers the per-thread encoder (Z <= 64, no
+    filler bits), the warp encoder (larger Z or filler bits), puncturing and
+    filler LLRs."""
+    import torch
+    from ldpc_b200 import codes
+    if name.endswith("bg1 z32"):   # Z = 32 without filler bits: the per-thread encoder with puncturing
+        code = codes.code_by_name(name.split()[0], bg=1, z=32)
+    else:
+        code = codes.code_by_name(name)
+    ctx = capi.Context(capi.Code.from_tables(code), max_iter=10, max_row_metric=31.0, beta=1.0, llr_scale=2.0,
+                       max_abs_llr=24.0)
+    snrs = np.array([-1.0, 0.5, 3.0], np.float32)
+    hw = ctx.info.hard_words
+    lf = torch.empty((len(snrs), n, code.n), dtype=torch.float32, device="cuda")
+    li = torch.empty((len(snrs), n, code.n), dtype=torch.int8, device="cuda")
+    d1 = torch.empty((n, hw), dtype=torch.int32, device="cuda")
+    d2 = torch.empty_like(d1)
+    u1 = torch.zeros(len(snrs), dtype=torch.int64, device="cuda")
+    u2 = torch.zeros_like(u1)
+    ctx.generate(77, 5000, snrs, n, llr_f32=lf, data_bits=d1, uncoded=u1)
+    ctx.generate(77, 5000, snrs, n, llr_i8=li, data_bits=d2, uncoded=u2)
+    torch.cuda.synchronize()
+    assert torch.equal(d1, d2)
+    assert torch.equal(u1, u2)
+    F = lf.cpu().numpy()
+    assert np.array_equal(li.cpu().numpy(), np.rint(F).astype(np.int16).astype(np.int8))
+    if code.punc_list:
+        assert np.all(F[:, :, code.punc_list[0]:code.punc_list[1] + 1] == 0)

@@ -48,3 +48,32 @@ def test_lines_match_simulate(capi, tmp_path, exe, name, params):
             assert abs(snr - snrs[k]) < 1e-5
             assert (inp, it, be, cwe) == (st_["uncoded_errors"], st_["iterations"], st_["bit_errors"], st_["cw_errors"])
             assert ticks > 0
+
+
+def test_resumed_run_equals_uninterrupted(tmp_path):
+    """A run stopped after two outer loops (its state file saved) and resumed
+    with four prints, loop for loop, the counters of one uninterrupted
+    four-loop run: the resumed loops continue at the saved codeword offset."""
+    from ldpc_b200 import codes
+    codes.make_code("11ad 1/2").write_dat(str(tmp_path / "e.dat"), str(tmp_path / "d.dat"))
+    seeds = [(0x9E3779B9 * (i + 3)) & ((1 << 56) - 1) for i in range(64)]
+    mk = lambda outer: blob(outer, 2, 3000, 10, 31.0, 2.0, 24.0, 1.0, -1.0, 0.0, 0.5, seeds, "e.dat", "d.dat")  # noqa: E731
+    exe = tmp_path / "LDPCtop_Vec64c_min_b200"
+    os.symlink(SIM, exe)
+
+    def run(outer, state=None):
+        env = dict(os.environ)
+        env.pop("LDPC_SIM_STATE", None)
+        if state:
+            env["LDPC_SIM_STATE"] = str(state)
+        r = subprocess.run([str(exe)], input=mk(outer), capture_output=True, timeout=300, cwd=tmp_path, env=env)
+        assert r.returncode == 0, r.stdout.decode()[-2000:]
+        return [l[:5] for l in parse(r.stdout.decode())["loops"]]
+
+    st = tmp_path / "run.state"
+    first = run(2, st)
+    assert st.exists() and len(first) == 2 * 3
+    resumed = run(4, st)
+    whole = run(4)
+    assert resumed[:6] == first
+    assert resumed == whole
