@@ -231,7 +231,7 @@ def hetero_mix(steps: int = 3, warmup: int = 1, total: int = 10_000_000, seed: i
     # converted to int8 LLR units (scale 2), rounded, and decoded as an int8
     # [iteration][layer] table
     t0 = time.time()
-    offsets = []
+    offsets, kept = [], []
     for ci, (h, c) in enumerate(zip(handles, objs)):
         fctx = capi.Context(h, variant=capi.LDPC_F32_OMS, max_iter=10, max_row_metric=31.0, beta=0.5,
                             llr_scale=1.0, max_abs_llr=1e9)
@@ -239,7 +239,17 @@ def hetero_mix(steps: int = 3, warmup: int = 1, total: int = 10_000_000, seed: i
         beta, _ = learned.train(fctx, c, iters=10, batch=8192, steps=train_steps, ebn0=(eb - 0.25, eb + 0.25), lr=0.02,
                                 init=0.5, seed=seed + ci, n_snr=4, quant_step=0.5)
         b8 = np.clip(np.rint(2.0 * beta.cpu().numpy()), 0, 127).astype(np.float32)   # [iters][layers]
-        batch.set_offset_table(ci, b8)
+        # deploy the table only when it beats the plain offset on fresh codewords: fewer
+        # iterations, codeword errors within two standard deviations of the plain count
+        vctx = capi.Context(h, max_iter=10)
+        plain_v = vctx.simulate(seed=seed + 1000 + ci, cw_offset=1 << 40, snr_db=[snr[ci]], n_per_snr=200_000)[0]
+        vctx.set_offset_table(b8)
+        tab_v = vctx.simulate(seed=seed + 1000 + ci, cw_offset=1 << 40, snr_db=[snr[ci]], n_per_snr=200_000)[0]
+        keep = (tab_v["iterations"] < plain_v["iterations"] and
+                tab_v["cw_errors"] <= plain_v["cw_errors"] + 2.0 * math.sqrt(max(plain_v["cw_errors"], 1)))
+        if keep:
+            batch.set_offset_table(ci, b8)
+        kept.append(bool(keep))
         offsets.append(b8.astype(int).tolist())
     train_s = time.time() - t0
     plan_l = batch.plan(specs)
@@ -262,6 +272,10 @@ def hetero_mix(steps: int = 3, warmup: int = 1, total: int = 10_000_000, seed: i
         "info_gbps": sum(m * c.k for m, c in zip(counts, objs)) / (avg_plain * 1e-3) / 1e9,
         "learned": {"value": total / (avg_learned * 1e-3), "unit": "codewords/s", "avg_iter": it_l,
                     "offsets_int8": dict(zip(names, offsets)), "training_s": round(train_s, 1),
+                    "deployed": dict(zip(names, kept)),
+                    "deploy_rule": "a code keeps its learned table only when, on 2e5 fresh codewords at its SNR, it "
+                                   "needs fewer iterations than the plain offset with codeword errors within two "
+                                   "standard deviations; otherwise the plain offset stays",
                     "training": "float offset min-sum, 10 iterations, %d Adam steps of 8192 codewords at the "
                                 "calibrated SNR +-0.25 dB, quantisation-aware (offsets rounded to multiples of 0.5, "
                                 "straight-through gradient); offsets x2 (int8 LLR scale) deployed as an int8 "
