@@ -130,9 +130,27 @@ int launch_gen(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* snr_
     job.uncoded = uncoded;
     GenTile tile;
     const size_t smem = gen_tile_shape(x->gent, &tile);
-    // int8 output alone, whole 4-element blocks, a clamp the rounding trick covers
+    // int8 output alone, whole 4-element blocks, a clamp bound the rounding trick covers
     tile.fast = (job.llr_i8 && !job.llr_f32 && !job.llr_i16 && !job.llr_i32 && !job.llr_f64 && (x->gent.n & 3) == 0 &&
-                 std::fabs(job.max_abs) < 2097152.0f && n_snr <= (size_t)GEN_FAST_SNR) ? 1 : 0;
+                 std::fabs(job.max_abs) < 32767.0f && n_snr <= (size_t)GEN_FAST_SNR) ? 1 : 0;
+    // the 16-bit clamp after rounding needs |rx * sf| < 2^15 before the clamp: |noise| <= 9.5 (the
+    // generator's largest Box-Muller radius), so |rx| <= 1 + 9.5 sigma
+    tile.clamp16 = 1;
+    for (size_t i = 0; i < n_snr; ++i)
+        if (!((1.0 + 9.5 * (double)job.sigma[i]) * (double)job.sigma_factor[i] < 32000.0)) tile.clamp16 = 0;
+    for (int r = 0; r < 10; ++r) {
+        job.philox_rk[2 * r] = (uint32_t)seed + (uint32_t)r * 0x9E3779B9u;
+        job.philox_rk[2 * r + 1] = (uint32_t)(seed >> 32) + (uint32_t)r * 0xBB67AE85u;
+    }
+    job.snr_stride = (long long)n_per_snr * x->gent.n;
+    // the fast path counts uncoded errors in byte counters folded once per tile:
+    // at most 255 items (4-bit blocks) per thread and tile
+    const int nb = (x->gent.n + 3) / 4;
+    if (tile.fast) {
+        if (nb > 255 * GEN_THREADS) tile.fast = 0;
+        else
+            while (tile.T > 1 && (long long)tile.T * nb > 255LL * GEN_THREADS) tile.T /= 2;
+    }
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)gen_kernel, GEN_THREADS, smem));
     const long long tiles = ((long long)n_per_snr + tile.T - 1) / tile.T;

@@ -15,8 +15,9 @@
 // stream 2 extends the Gaussian tail.  Gaussians come from the Box-Muller
 // transform r = sqrt(-2 ln u1), (r cos 2 pi u2, r sin 2 pi u2) with
 // u1 = (w + 1/2) 2^-32; when w < 256 a second word refines u1 down to 2^-65,
-// so samples reach ~9.4 sigma (the reference's generator reaches ~9.3 sigma,
-// docs/WGN/norm.dist.methods.html).  The same noise is reused for every SNR
+// so samples reach ~9.5 sigma (the reference's generator reaches ~9.3 sigma,
+// docs/WGN/norm.dist.methods.html).  log2, sqrt and sin/cos are the hardware
+// approximations (box_muller_fast); the noise is checked statistically.  The same noise is reused for every SNR
 // point, as the reference's inner loop does (src/Top/LDPCtop.cpp:89-97).
 #pragma once
 #include <stdint.h>
@@ -37,26 +38,22 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
     return c;
 }
 
+// The same generator with its ten round keys precomputed (GenJob::philox_rk):
+// each key is an operand read from the kernel parameters, not recomputed.
+__device__ __forceinline__ uint4 philox_rk(uint64_t cw, uint32_t block, uint32_t stream, const uint32_t (&rk)[20]) {
+    uint4 c = make_uint4((uint32_t)cw, (uint32_t)(cw >> 32), block, stream);
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+        const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = make_uint4(hi1 ^ c.y ^ rk[2 * r], lo1, hi0 ^ c.w ^ rk[2 * r + 1], lo0);
+    }
+    return c;
+}
+
 __device__ __forceinline__ uint4 philox_at(uint64_t seed, uint64_t cw, uint32_t block, uint32_t stream) {
     return philox4x32_10(make_uint4((uint32_t)cw, (uint32_t)(cw >> 32), block, stream),
                          make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
-}
-
-// One Box-Muller pair from two 32-bit words (and a refinement word pair for the tail).
-__device__ __forceinline__ float2 box_muller(uint32_t w_r, uint32_t w_a, uint64_t seed, uint64_t cw, uint32_t block,
-                                             int which) {
-    float u1;
-    if (w_r < 256u) {
-        const uint4 x = philox_at(seed, cw, block, 2u);
-        const uint32_t w2 = which ? x.z : x.x;
-        u1 = fmaf((float)w_r, 0x1p-32f, fmaf((float)w2, 0x1p-64f, 0x1p-65f));
-    } else {
-        u1 = fmaf((float)w_r, 0x1p-32f, 0x1p-33f);
-    }
-    const float r = sqrtf(-2.0f * logf(u1));
-    float s, c;
-    sincospif((float)w_a * 0x1p-31f, &s, &c);   // angle 2*pi*w_a/2^32
-    return make_float2(r * c, r * s);
 }
 
 // gen_metrics for one element: returns 1 for an uncoded sign error.
@@ -225,11 +222,11 @@ __device__ void gen_encode_thread(const GenTables& tb, const uint32_t* dat, uint
 // sin/cos (absolute errors ~2^-21; the noise is checked statistically).
 // u1 = (w_r + 1/2) 2^-32, refined by a second word down to 2^-65 when
 // w_r < 256 (tail to ~9.5 sigma); angle = pi * (int)w_a * 2^-31 in [-pi, pi).
-__device__ __forceinline__ float2 box_muller_fast(uint32_t w_r, uint32_t w_a, uint64_t seed, uint64_t cw,
+__device__ __forceinline__ float2 box_muller_fast(uint32_t w_r, uint32_t w_a, const uint32_t (&rk)[20], uint64_t cw,
                                                   uint32_t block, int which) {
     float u1;
     if (w_r < 256u) {
-        const uint4 x = philox_at(seed, cw, block, 2u);
+        const uint4 x = philox_rk(cw, block, 2u, rk);
         const uint32_t w2 = which ? x.z : x.x;
         u1 = fmaf((float)w_r, 0x1p-32f, fmaf((float)w2, 0x1p-64f, 0x1p-65f));
     } else {
@@ -261,21 +258,30 @@ __device__ __forceinline__ uint32_t sign_bytes4(float x0, float x1, float x2, fl
 struct GenTile {
     int T;              // codewords per tile
     int thread_enc;     // 1: gen_encode_thread, 0: encode_warp
-    int fast;           // 1: int8 output only, n % 4 == 0, |max_abs| < 2^21, at most GEN_FAST_SNR points
+    int fast;           // 1: int8 output only, n % 4 == 0, |max_abs| < 2^15, at most GEN_FAST_SNR points
+    int clamp16;        // fast path: |rx * sf| < 2^15 at every SNR point, clamp on 16-bit pairs after rounding
 };
 constexpr int GEN_FAST_SNR = 8;
 
 // gen_metrics for four elements at every SNR point, the int8 output only:
-// rx = fma(noise, sigma, orig), l = rx * sf, clamp to [-max_abs, max_abs]
-// (these three steps as llr_element does them), then round-half-even by
-// adding 1.5 * 2^23 (exact for |l| < 2^21) and keeping the low byte, which
-// is (int8)(int16)roundi(l).  Punctured elements give 0, filler elements
-// roundi(max_abs).  The uncoded error of an element is the sign of rx
-// against the sent sign; counts go to unc[s] (8 x the count: one bit per
-// byte of a sign mask, divided out at the end).
-__device__ __forceinline__ void llr4_i8_fast(const GenJob& job, long long i, long long row_stride, int idx0,
-                                             const float (&nz)[4], uint32_t bits4, uint32_t pmask, uint32_t fmask,
-                                             uint32_t fbytes, unsigned (&unc)[GEN_FAST_SNR]) {
+// rx = fma(noise, sigma, orig) and l = rx * sf as llr_element computes them,
+// then the clamp to [-max_abs, max_abs] and roundi: adding 1.5 * 2^23 rounds
+// half-even exactly for |l| < 2^21 and leaves roundi(l) in the low bits.
+// With clamp16 (the host has bounded |l| < 2^15 at every SNR point) the clamp
+// runs after the rounding, on 16-bit lane pairs against +-roundi(max_abs)
+// (roundi is monotone, so clamp-then-round equals round-then-clamp to the
+// rounded bounds); otherwise it runs on the floats, as llr_element does.
+// The low byte of each lane is (int8)(int16)roundi(l).  Punctured elements
+// give 0, filler elements roundi(max_abs).  The uncoded error of an element
+// is the sign of rx against the sent sign; counts go to unc[s] as four byte
+// counters (one per element of the word), which the kernel folds at the end
+// of every tile (the host keeps a thread's items per tile below 256).
+__device__ __forceinline__ uint32_t vmax_s16x2(uint32_t a, uint32_t b) { uint32_t d; asm("max.s16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); return d; }
+__device__ __forceinline__ uint32_t vmin_s16x2(uint32_t a, uint32_t b) { uint32_t d; asm("min.s16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); return d; }
+
+__device__ __forceinline__ void llr4_i8_fast(const GenJob& job, int8_t* dst, bool clamp16, const float (&nz)[4],
+                                             uint32_t bits4, uint32_t pmask, uint32_t fmask, uint32_t fbytes,
+                                             uint32_t lo2, uint32_t hi2, unsigned (&unc)[GEN_FAST_SNR]) {
     float o[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) o[q] = ((bits4 >> q) & 1u) ? -1.0f : 1.0f;
@@ -291,19 +297,29 @@ __device__ __forceinline__ void llr4_i8_fast(const GenJob& job, long long i, lon
             for (int q = 0; q < 4; ++q) {
                 rx[q] = fmaf(nz[q], sg, o[q]);
                 float l = __fmul_rn(rx[q], sf);
-                l = ma < l ? ma : l;
-                l = -ma > l ? -ma : l;
+                if (!clamp16) {
+                    l = ma < l ? ma : l;
+                    l = -ma > l ? -ma : l;
+                }
                 t[q] = __float_as_uint(__fadd_rn(l, 12582912.0f));
             }
-            uint32_t packed = __byte_perm(__byte_perm(t[0], t[1], 0x0040), __byte_perm(t[2], t[3], 0x0040), 0x5410);
+            uint32_t packed;
+            if (clamp16) {
+                const uint32_t p01 = vmin_s16x2(vmax_s16x2(__byte_perm(t[0], t[1], 0x5410), lo2), hi2);
+                const uint32_t p23 = vmin_s16x2(vmax_s16x2(__byte_perm(t[2], t[3], 0x5410), lo2), hi2);
+                packed = __byte_perm(p01, p23, 0x6420);
+            } else {
+                packed = __byte_perm(__byte_perm(t[0], t[1], 0x0040), __byte_perm(t[2], t[3], 0x0040), 0x5410);
+            }
             packed = (packed & ~(pmask | fmask)) | (fbytes & fmask);
-            *reinterpret_cast<uint32_t*>(job.llr_i8 + ((long long)s * job.n_per_snr + i) * row_stride + idx0) = packed;
-            unc[s] += __popc(sign_bytes4(rx[0], rx[1], rx[2], rx[3]) ^ osign);
+            *reinterpret_cast<uint32_t*>(dst) = packed;
+            dst += job.snr_stride;
+            unc[s] += (sign_bytes4(rx[0], rx[1], rx[2], rx[3]) ^ osign) & 0x01010101u;
         }
     }
 }
 
-__global__ void __launch_bounds__(GEN_THREADS) gen_kernel(const __grid_constant__ GenTables tb,
+__global__ void __launch_bounds__(GEN_THREADS, 4) gen_kernel(const __grid_constant__ GenTables tb,
                                                           const __grid_constant__ GenJob job, const GenTile tile) {
     extern __shared__ __align__(16) uint32_t sm[];
     __shared__ unsigned long long s_unc[GEN_MAX_SNR];
@@ -328,7 +344,7 @@ __global__ void __launch_bounds__(GEN_THREADS) gen_kernel(const __grid_constant_
             if (tid < tc) {
                 const uint64_t cw = job.cw_offset + (uint64_t)(i0 + tid);
                 for (int b = 0; 4 * b < dwp; ++b) {
-                    const uint4 x = philox_at(job.seed, cw, (uint32_t)b, 0u);
+                    const uint4 x = philox_rk(cw, (uint32_t)b, 0u, job.philox_rk);
                     const uint32_t v[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
@@ -361,13 +377,19 @@ __global__ void __launch_bounds__(GEN_THREADS) gen_kernel(const __grid_constant_
         __syncthreads();
         // ---- phase B: noise and LLRs, item f = codeword c, block b of 4 bits ----
         const long long row_stride = tb.n;
-        for (int f = tid; f < tc * nb; f += GEN_THREADS) {
-            const int c = f / nb, b = f - c * nb;
+        // (c, b) of item f advanced by GEN_THREADS items per step, without a division per item
+        int c = tid / nb, b = tid - (tid / nb) * nb;
+        const int step_c = GEN_THREADS / nb, step_b = GEN_THREADS - step_c * nb;
+        for (int f = tid; f < tc * nb; f += GEN_THREADS, c += step_c, b += step_b) {
+            if (b >= nb) {
+                b -= nb;
+                ++c;
+            }
             const long long i = i0 + c;
             const uint64_t cw = job.cw_offset + (uint64_t)i;
-            const uint4 x = philox_at(job.seed, cw, (uint32_t)b, 1u);
-            const float2 g0 = box_muller_fast(x.x, x.y, job.seed, cw, (uint32_t)b, 0);
-            const float2 g1 = box_muller_fast(x.z, x.w, job.seed, cw, (uint32_t)b, 1);
+            const uint4 x = philox_rk(cw, (uint32_t)b, 1u, job.philox_rk);
+            const float2 g0 = box_muller_fast(x.x, x.y, job.philox_rk, cw, (uint32_t)b, 0);
+            const float2 g1 = box_muller_fast(x.z, x.w, job.philox_rk, cw, (uint32_t)b, 1);
             const float nz[4] = {g0.x, g0.y, g1.x, g1.y};
             const int idx0 = 4 * b;
             const uint32_t bits4 = (bits[(idx0 >> 5) * T + c] >> (idx0 & 31)) & 0xfu;
@@ -375,8 +397,10 @@ __global__ void __launch_bounds__(GEN_THREADS) gen_kernel(const __grid_constant_
                 uint32_t pmask = 0u, fmask = 0u;
                 if (tb.any_punct) pmask = *reinterpret_cast<const uint32_t*>(tb.punct + idx0) * 0xffu;
                 if (tb.any_filler) fmask = *reinterpret_cast<const uint32_t*>(tb.filler + idx0) * 0xffu;
-                const uint32_t fbyte = (uint32_t)__float2int_rn(job.max_abs) & 0xffu;
-                llr4_i8_fast(job, i, row_stride, idx0, nz, bits4, pmask, fmask, fbyte * 0x01010101u, unc_f);
+                const int m = __float2int_rn(job.max_abs);
+                const uint32_t hi2 = ((uint32_t)m & 0xffffu) * 0x10001u, lo2 = ((uint32_t)(-m) & 0xffffu) * 0x10001u;
+                llr4_i8_fast(job, job.llr_i8 + i * row_stride + idx0, tile.clamp16, nz, bits4, pmask, fmask,
+                             ((uint32_t)m & 0xffu) * 0x01010101u, lo2, hi2, unc_f);
                 continue;
             }
             for (int s = 0; s < job.n_snr; ++s) {
@@ -424,20 +448,19 @@ __global__ void __launch_bounds__(GEN_THREADS) gen_kernel(const __grid_constant_
                 }
             }
         }
-    }
-    if (job.uncoded) {
-        if (tile.fast) {
-            // each error counted 8 times (one per bit of a 0xff byte)
+        if (tile.fast && job.uncoded) {
+            // fold the byte counters of this tile (each byte < 256)
 #pragma unroll
             for (int s = 0; s < GEN_FAST_SNR; ++s) {
                 if (s < job.n_snr) {
-                    unsigned long long v = unc_f[s] >> 3;
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                    if (lane == 0 && v) atomicAdd(&s_unc[s], v);
+                    const unsigned v = __dp4a(unc_f[s], 0x01010101u, 0u);
+                    if (v) atomicAdd(&s_unc[s], (unsigned long long)v);
+                    unc_f[s] = 0;
                 }
             }
         }
+    }
+    if (job.uncoded) {
         __syncthreads();
         for (int s = tid; s < job.n_snr; s += blockDim.x)
             if (s_unc[s]) atomicAdd(job.uncoded + s, s_unc[s]);

@@ -25,7 +25,7 @@
 //
 // Work layout (one CTA, persistent):
 //   G groups x 2 lanes = 2G codeword slots.  Thread (t, g) = check row t of
-//   every layer for group g; tid = t*G + g.  Posteriors of group g live in
+//   every layer for group g; tid = g*Z + t.  Posteriors of group g live in
 //   shared memory at Ps[g*stride + c*Z + v] (stride chosen so a warp's
 //   accesses fall in distinct banks).  Check messages R stay in registers,
 //   R[l][j] = edge slot j of layer l for this thread's check row.
@@ -361,8 +361,11 @@ __global__ void __launch_bounds__(MAXT, MINB) oms_f16_kernel(const __grid_consta
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const int nwarps = blockDim.x >> 5;
-    const int t = tid / G, g = tid - (tid / G) * G;
-    const bool active = t < z;
+    // thread tid = g * z + t: a warp holds consecutive rows of one or two
+    // codeword pairs (consecutive posterior words, one bank each); measured
+    // 0.5 % faster than interleaving the pairs (tid = t * G + g)
+    const int g = tid / z, t = tid - (tid / z) * z;
+    const bool active = g < G;
     const int gbase = g * stride;
     // this CTA's contiguous share of the codewords (static: no global atomics)
     const long long lo = job.ncw * blockIdx.x / gridDim.x, hi = job.ncw * (blockIdx.x + 1) / gridDim.x;

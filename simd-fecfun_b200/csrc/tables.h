@@ -164,6 +164,8 @@ struct GenJob {
     float* llr_f32;                  // [n_snr][n_per_snr][n] or null
     uint32_t* data_bits;             // [n_per_snr][hard_words] or null
     unsigned long long* uncoded;     // [n_snr] or null
+    uint32_t philox_rk[20];          // Philox round keys of `seed`: (lo, hi) + r * (0x9E3779B9, 0xBB67AE85), r = 0..9
+    long long snr_stride;            // elements between SNR rows: n_per_snr * n
 };
 
 }  // namespace ldpc
