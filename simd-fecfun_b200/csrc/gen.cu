@@ -89,7 +89,8 @@ int setup_gen(ldpc_ctx* x) {
     GenTile tile;
     const size_t gsmem = gen_tile_shape(t, &tile);
     if (gsmem > 200 * 1024) return fail(LDPC_ERR_UNSUPPORTED, "generator tile needs %zu B of shared memory", gsmem);
-    CUDA_TRY(allow_dynamic_smem((const void*)gen_kernel, 200 * 1024));
+    CUDA_TRY(allow_dynamic_smem((const void*)gen_kernel<false>, 200 * 1024));
+    CUDA_TRY(allow_dynamic_smem((const void*)gen_kernel<true>, 200 * 1024));
     CUDA_TRY(allow_dynamic_smem((const void*)encode_kernel, 200 * 1024));
     return LDPC_OK;
 }
@@ -151,11 +152,14 @@ int launch_gen(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* snr_
         else
             while (tile.T > 1 && (long long)tile.T * nb > 255LL * GEN_THREADS) tile.T /= 2;
     }
+    const bool pf = x->gent.any_punct || x->gent.any_filler;
+    const void* kfn = pf ? (const void*)gen_kernel<true> : (const void*)gen_kernel<false>;
     int per_sm = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)gen_kernel, GEN_THREADS, smem));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, GEN_THREADS, smem));
     const long long tiles = ((long long)n_per_snr + tile.T - 1) / tile.T;
     const int grid = (int)std::max<long long>(1, std::min<long long>(tiles, (long long)x->sms * std::max(per_sm, 1)));
-    gen_kernel<<<grid, GEN_THREADS, smem, s>>>(x->gent, job, tile);
+    if (pf) gen_kernel<true><<<grid, GEN_THREADS, smem, s>>>(x->gent, job, tile);
+    else gen_kernel<false><<<grid, GEN_THREADS, smem, s>>>(x->gent, job, tile);
     CUDA_TRY(cudaGetLastError());
     return LDPC_OK;
 }

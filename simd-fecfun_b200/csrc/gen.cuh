@@ -311,7 +311,7 @@ __device__ __forceinline__ void llr4_i8_fast(const GenJob& job, int8_t* dst, boo
             } else {
                 packed = __byte_perm(__byte_perm(t[0], t[1], 0x0040), __byte_perm(t[2], t[3], 0x0040), 0x5410);
             }
-            packed = (packed & ~(pmask | fmask)) | (fbytes & fmask);
+            if (pmask | fmask) packed = (packed & ~(pmask | fmask)) | (fbytes & fmask);
             *reinterpret_cast<uint32_t*>(dst) = packed;
             dst += job.snr_stride;
             unc[s] += (sign_bytes4(rx[0], rx[1], rx[2], rx[3]) ^ osign) & 0x01010101u;
@@ -319,6 +319,9 @@ __device__ __forceinline__ void llr4_i8_fast(const GenJob& job, int8_t* dst, boo
     }
 }
 
+// PF: the code has punctured or filler bits (their masks are applied in the
+// int8 path only then).
+template <bool PF>
 __global__ void __launch_bounds__(GEN_THREADS, 4) gen_kernel(const __grid_constant__ GenTables tb,
                                                           const __grid_constant__ GenJob job, const GenTile tile) {
     extern __shared__ __align__(16) uint32_t sm[];
@@ -395,8 +398,8 @@ __global__ void __launch_bounds__(GEN_THREADS, 4) gen_kernel(const __grid_consta
             const uint32_t bits4 = (bits[(idx0 >> 5) * T + c] >> (idx0 & 31)) & 0xfu;
             if (tile.fast) {
                 uint32_t pmask = 0u, fmask = 0u;
-                if (tb.any_punct) pmask = *reinterpret_cast<const uint32_t*>(tb.punct + idx0) * 0xffu;
-                if (tb.any_filler) fmask = *reinterpret_cast<const uint32_t*>(tb.filler + idx0) * 0xffu;
+                if (PF && tb.any_punct) pmask = *reinterpret_cast<const uint32_t*>(tb.punct + idx0) * 0xffu;
+                if (PF && tb.any_filler) fmask = *reinterpret_cast<const uint32_t*>(tb.filler + idx0) * 0xffu;
                 const int m = __float2int_rn(job.max_abs);
                 const uint32_t hi2 = ((uint32_t)m & 0xffffu) * 0x10001u, lo2 = ((uint32_t)(-m) & 0xffffu) * 0x10001u;
                 llr4_i8_fast(job, job.llr_i8 + i * row_stride + idx0, tile.clamp16, nz, bits4, pmask, fmask,

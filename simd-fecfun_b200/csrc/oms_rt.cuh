@@ -138,6 +138,113 @@ __device__ __forceinline__ void rt_syndrome(const RtCode& C, const uint32_t* Ps,
 // Shared memory: [RtCode copy][posteriors G x stride words][LLR staging 2G x nstage bytes][messages (E | 1) x blockDim words if RSMEM]
 __host__ __device__ constexpr int rt_code_bytes() { return (int)((sizeof(RtCode) + 15) & ~(size_t)15); }
 
+// Slot phase with the whole CTA on each finished codeword (used when the CTA
+// has more warps than codeword slots, where one warp per slot would leave the
+// others idle: 5G NR and other long codes).  Every thread derives the same
+// set of finished slots from shared state.  Element i of a codeword belongs to
+// thread i mod blockDim: that thread reads its finished posterior (hard bit,
+// error, posterior out) and then writes the next codeword's LLR there, so no
+// element is read by one thread and overwritten by another; warp w's lanes
+// hold elements 32 (w + m nwarps) + lane, one hard-decision word per ballot.
+// Then, after a barrier, warp k mod nwarps does slot k's bookkeeping, claim
+// and prefetch.  Entered after a barrier that follows every thread's
+// cp.async wait; the caller commits the prefetches and ends with a barrier.
+__device__ __forceinline__ void rt_slots_coop(const RtCode& C, const RtJob& job, uint32_t* Ps, int8_t* stage_base, int stride,
+                                           int nstage, int nslots, long long hi, int par, long long* s_cur,
+                                           long long* s_next, int* s_it, uint32_t (*s_synd)[16],
+                                           uint32_t (*s_zero_mask)[16], int* s_busy, unsigned long long& s_head,
+                                           unsigned long long (*s_cnt)[4], unsigned* s_err_bits, unsigned* s_err_slots) {
+    const int tid = threadIdx.x, nthr = blockDim.x, warp = tid >> 5, lane = tid & 31, nwarps = nthr >> 5;
+    const int n = C.n, z = C.z;
+    unsigned fin = 0;
+    for (int k = 0; k < nslots; ++k) {
+        if (s_cur[k] < 0) continue;
+        const uint32_t bit = (k & 1) ? 0x80000000u : 0x00008000u;
+        if (!(s_synd[par][k >> 1] & bit) || s_it[k] + 1 >= C.max_iter) fin |= 1u << k;
+    }
+    for (unsigned f = fin; f; f &= f - 1) {
+        const int k = __ffs(f) - 1;
+        const long long cw = s_cur[k];
+        __half* pk = reinterpret_cast<__half*>(Ps + (k >> 1) * stride) + (k & 1);
+        const uint32_t* ref = job.ref_bits ? job.ref_bits + (cw % job.ref_period) * C.hard_words : nullptr;
+        unsigned errw = 0, errslots = 0;
+        for (int i0 = warp * 32; i0 < C.kbits; i0 += nthr) {
+            const int i = i0 + lane;
+            const bool b = (i < C.kbits) && __hlt(pk[2 * i], __float2half(0.0f));
+            const uint32_t word = __ballot_sync(0xffffffffu, b);
+            if (lane == 0 && job.hard_out) job.hard_out[cw * C.hard_words + (i0 >> 5)] = word;
+            if (ref) {
+                uint32_t e = word ^ ref[i0 >> 5];
+                if (i0 + 32 > C.kbits) e &= (1u << (C.kbits - i0)) - 1u;
+                errw += __popc(e);
+                if ((e >> lane) & 1u) errslots |= 1u << ((i % z) % C.num_par);
+            }
+        }
+        if (ref && job.counters) {
+            errslots = __reduce_or_sync(0xffffffffu, errslots);
+            if (lane == 0 && errw) {
+                atomicAdd(&s_err_bits[k], errw);
+                atomicOr(&s_err_slots[k], errslots);
+            }
+        }
+        if (job.post_out) {
+            int8_t* dst = job.post_out + cw * (long long)n;
+            for (int i = tid; i < n; i += nthr) dst[i] = (int8_t)__half2int_rn(pk[2 * i]);
+        }
+        if (s_next[k] >= 0) {
+            const int8_t* st = stage_base + k * nstage;
+            for (int i = tid; i < n; i += nthr) pk[2 * i] = __int2half_rn((int)st[i]);
+        }
+    }
+    // every thread has taken its decision from s_cur / s_it / s_synd, summed its
+    // errors and read the staging buffers before the bookkeeping changes them
+    __syncthreads();
+    for (int k = warp; k < nslots; k += nwarps) {
+        const long long cw = s_cur[k];
+        if (cw < 0) continue;
+        const int it = s_it[k] + 1;
+        if (!((fin >> k) & 1u)) {
+            if (lane == 0) {
+                s_it[k] = it;
+                s_busy[par] = 1;
+            }
+            continue;
+        }
+        const long long nxt = s_next[k];
+        unsigned long long c = 0;
+        if (lane == 0) {
+            if (job.iters_out) job.iters_out[cw] = (uint8_t)it;
+            if (job.counters) {
+                int bk = (int)(cw / job.bucket_size);
+                bk = bk < job.n_buckets ? bk : job.n_buckets - 1;
+                atomicAdd(&s_cnt[bk][0], 1ull);
+                atomicAdd(&s_cnt[bk][1], (unsigned long long)it);
+                if (s_err_bits[k]) {
+                    atomicAdd(&s_cnt[bk][2], (unsigned long long)s_err_bits[k]);
+                    atomicAdd(&s_cnt[bk][3], (unsigned long long)__popc(s_err_slots[k]));
+                    s_err_bits[k] = 0;
+                    s_err_slots[k] = 0;
+                }
+            }
+            if (nxt >= 0) c = atomicAdd(&s_head, 1ull);
+        }
+        if (nxt >= 0) {
+            c = __shfl_sync(0xffffffffu, c, 0);
+            const long long fresh = (long long)c < hi ? (long long)c : -1;
+            if (fresh >= 0) prefetch_llr(stage_base + k * nstage, job.llr, fresh, n, lane);
+            if (lane == 0) {
+                s_next[k] = fresh;
+                s_busy[par] = 1;
+            }
+        }
+        if (lane == 0) {
+            s_cur[k] = nxt;
+            s_it[k] = 0;
+            atomicOr(&s_zero_mask[par][k >> 1], (k & 1) ? 0xffff0000u : 0x0000ffffu);
+        }
+    }
+}
+
 template <int DMAX, bool QUIRK, bool RSMEM>
 __global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtLaunch lp) {
     extern __shared__ __align__(16) unsigned char rt_smem[];
@@ -150,6 +257,7 @@ __global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtL
     __shared__ unsigned long long s_head;
     __shared__ unsigned long long s_cnt[OMS_MAX_BUCKETS][4];
     __shared__ int s_code_idx;
+    __shared__ unsigned s_err_bits[32], s_err_slots[32];   // cooperative write-out: per slot error sums
 
     const RtCode& C = *reinterpret_cast<const RtCode*>(rt_smem);
     uint32_t* const Ps = reinterpret_cast<uint32_t*>(rt_smem + rt_code_bytes());
@@ -214,6 +322,7 @@ __global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtL
             s_cur[tid] = ok && c0 < hi ? c0 : -1;
             s_next[tid] = ok && c1 < hi ? c1 : -1;
             s_it[tid] = 0;
+            s_err_bits[tid] = s_err_slots[tid] = 0;
             if (tid < 16) {
                 s_synd[0][tid] = s_synd[1][tid] = 0;
                 s_zero_mask[0][tid] = s_zero_mask[1][tid] = 0;
@@ -254,11 +363,16 @@ __global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtL
             }
             if (tid == 0) s_busy[par ^ 1] = 0;
             if (active) rt_syndrome<DMAX>(C, Ps, t, gbase, z, &s_synd[par][g]);
-            __syncthreads();
+            cp_async_wait_all();   // this thread's prefetches (issued in an earlier slot phase)
+            __syncthreads();       // syndrome bits final, every prefetched byte visible
 
+            if (nslots < nwarps) {
+                // ------- more warps than slots (large codes): the whole CTA writes each
+                // finished codeword out and refills its slot -------
+                rt_slots_coop(C, job, Ps, stage_base, stride, nstage, nslots, hi, par, s_cur, s_next, s_it, s_synd,
+                              s_zero_mask, s_busy, s_head, s_cnt, s_err_bits, s_err_slots);
+            } else
             // ------- each warp: its slots -- decide, write out, promote, claim, prefetch -------
-            cp_async_wait_all();
-            __syncwarp();
             for (int k = warp; k < nslots; k += nwarps) {
                 const long long cw = s_cur[k];
                 if (cw < 0) continue;
