@@ -391,6 +391,15 @@ def run_workload(args):
         out = run_variants(args, clk)
     elif args.workload == "sim":
         out = run_sim(args)
+    elif args.workload == "op-rates":
+        from ldpc_b200 import capi
+        rates = capi.probe_op_rates(local)
+        fma, mufu = capi.probe_fp32_peak(local)
+        out = {"metric": "thread-level operations per clock per SM (eight independent chains per thread)",
+               "value": None, "unit": "ops/clk/SM", "n_gpus": 1, "dtype": "packed int8/int16/f16 and f32",
+               "rates": {k: round(v, 2) for k, v in rates},
+               "int32_ops_per_s": capi.probe_int32_peak(local), "fp32_fma_per_s": fma, "mufu_per_s": mufu,
+               "gpu_launches": None}
     elif args.workload == "offset-search":
         out = workloads.offset_search(n_search=args.search_n, n_valid=args.search_valid_n)
     else:
@@ -420,7 +429,8 @@ def main():
     ap.add_argument("--variant-ref-sample", type=int, default=4000,
                     help="int8 codewords per host thread for the reference builds (--workload variants)")
     ap.add_argument("--workload", default="11ad",
-                    choices=["11ad", "nr-mix", "hetero-mix", "learned", "sp-sweep", "variants", "sim", "offset-search"],
+                    choices=["11ad", "nr-mix", "hetero-mix", "learned", "sp-sweep", "variants", "sim", "offset-search",
+                             "op-rates"],
                     help="11ad: the headline run; others: the batched 5G NR mix, the 18-code 802.11 mix "
                          "(plain vs learned offsets), learned-offset training, the float sum-product Z sweep, "
                          "every decoder variant on the headline point, the process-level drop-in against the "

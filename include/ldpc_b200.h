@@ -410,6 +410,14 @@ int ldpc_probe_int32_peak(int device, double *ops_per_s);
  * No counterpart in the reference. */
 int ldpc_probe_fp32_peak(int device, double *fma_per_s, double *mufu_per_s);
 
+/* Thread-level throughput (operations per clock per SM, at the device's
+ * reported maximum clock) of single operations on packed lanes: int8x4 and
+ * int16x2 SIMD intrinsics, s16x2 / f16x2 / f32 instructions, prmt, lop3 --
+ * the measurements behind the int8 decoder's choice of f16x2 arithmetic.
+ * Fills the first min(n_ops, 17) entries; names[i] (optional) receives a
+ * static string naming operation i.  No counterpart in the reference. */
+int ldpc_probe_op_rates(int device, double *ops_per_clk_sm, int n_ops, const char **names);
+
 #ifdef __cplusplus
 }
 #endif

@@ -2,6 +2,7 @@
 // roofline.  Each thread runs eight interleaved chains of one 32-bit logic op
 // (lop3) or add (iadd3); inline PTX keeps the compiler from folding them.
 #include <algorithm>
+#include <utility>
 
 #include "internal.h"
 
@@ -49,6 +50,49 @@ __global__ void fp_peak_kernel(float* out, int iters, float seed) {
     float r = 0.f;
 #pragma unroll
     for (int c = 0; c < 8; ++c) r += x[c];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = r;
+}
+
+// Throughput of single operations on packed lanes, the measurements behind
+// the int8 decoder's choice of f16x2 arithmetic: each thread runs eight
+// independent chains of one operation.  OP indexes kOpNames.
+__device__ __forceinline__ uint32_t op_apply(int op, uint32_t a, uint32_t b) {
+    uint32_t d = a;
+    switch (op) {
+        case 0: d = __vsubss4(a, b); break;
+        case 1: d = __vaddss4(a, b); break;
+        case 2: d = __vabsss4(a) ^ b; break;
+        case 3: d = __vmins4(a, b); break;
+        case 4: d = __vsub4(a, b); break;
+        case 5: d = __vsubss2(a, b); break;
+        case 6: asm("min.s16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); break;
+        case 7: asm("add.s16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); break;
+        case 8: asm("min.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); break;
+        case 9: asm("add.rn.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); break;
+        case 10: asm("fma.rn.f16x2 %0, %1, %2, %1;" : "=r"(d) : "r"(a), "r"(b)); break;
+        case 11: asm("min.xorsign.abs.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); break;
+        case 12: asm("set.eq.u32.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); d ^= a; break;
+        case 13: d = __float_as_uint(fminf(__uint_as_float(a), __uint_as_float(b))); break;
+        case 14: d = __float_as_uint(__fadd_rn(__uint_as_float(a), __uint_as_float(b))); break;
+        case 15: d = __byte_perm(a, b, 0x5410); break;
+        default: asm("lop3.b32 %0, %1, %2, %1, 0x96;" : "=r"(d) : "r"(a), "r"(b)); break;
+    }
+    return d;
+}
+
+template <int OP>
+__global__ void op_rate_kernel(uint32_t* out, int iters, uint32_t seed) {
+    uint32_t x[8];
+    const uint32_t y = 0x3c003c00u ^ (threadIdx.x & 7);   // 1.0 in both f16 lanes, perturbed
+#pragma unroll
+    for (int c = 0; c < 8; ++c) x[c] = 0x40004000u + seed + c;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) x[c] = op_apply(OP, x[c], y);
+    }
+    uint32_t r = 0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) r ^= x[c];
     out[blockIdx.x * blockDim.x + threadIdx.x] = r;
 }
 
@@ -128,5 +172,44 @@ extern "C" int ldpc_probe_int32_peak(int device, double* ops_per_s) {
     cudaFree(out);
     CUDA_TRY(cudaGetLastError());
     *ops_per_s = best;
+    return LDPC_OK;
+}
+
+namespace {
+const char* const kOpNames[] = {"vsubss4 (int8x4 saturating sub)", "vaddss4", "vabsss4", "vmins4", "vsub4 (wrapping)",
+                                "vsubss2 (int16x2 saturating sub)", "min.s16x2", "add.s16x2", "min.f16x2",
+                                "add.rn.f16x2", "fma.rn.f16x2", "min.xorsign.abs.f16x2", "set.eq.u32.f16x2",
+                                "fmin (f32)", "add.rn.f32", "prmt", "lop3"};
+constexpr int kNumOps = 17;
+
+template <int... Ops>
+void launch_op(int op, int blocks, int threads, uint32_t* out, int iters, uint32_t seed, std::integer_sequence<int, Ops...>) {
+    ((op == Ops ? (ldpc::op_rate_kernel<Ops><<<blocks, threads>>>(out, iters, seed), 0) : 0), ...);
+}
+}  // namespace
+
+extern "C" int ldpc_probe_op_rates(int device, double* ops_per_clk_sm, int n_ops, const char** names) {
+    if (!ops_per_clk_sm || n_ops < 0) return fail(LDPC_ERR_INVALID_ARG, "NULL argument");
+    if (n_ops > kNumOps) n_ops = kNumOps;
+    CUDA_TRY(cudaSetDevice(device));
+    int sms = 0, clk_khz = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    CUDA_TRY(cudaDeviceGetAttribute(&clk_khz, cudaDevAttrClockRate, device));
+    const int threads = 256, blocks = sms * 8, iters = 4096;
+    uint32_t* out = nullptr;
+    CUDA_TRY(cudaMalloc(&out, sizeof(uint32_t) * threads * blocks));
+    for (int op = 0; op < n_ops; ++op) {
+        const double ops = (double)threads * blocks * iters * 8;
+        const double r = ldpc::time_ops(
+            [&](int rep) { launch_op(op, blocks, threads, out, iters, 17u + rep, std::make_integer_sequence<int, kNumOps>()); },
+            ops);
+        if (r < 0) {
+            cudaFree(out);
+            return fail(LDPC_ERR_CUDA, "op-rate probe kernel %d failed", op);
+        }
+        ops_per_clk_sm[op] = r / ((double)sms * clk_khz * 1e3);
+        if (names) names[op] = kOpNames[op];
+    }
+    cudaFree(out);
     return LDPC_OK;
 }

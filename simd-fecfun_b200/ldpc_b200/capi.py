@@ -98,6 +98,7 @@ _PROTOS = {
     "ldpc_decode_count": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _sz, _sz, _vp, C.c_int, _vp]),
     "ldpc_probe_int32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     "ldpc_probe_fp32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "ldpc_probe_op_rates": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_char_p)]),
     "ldpc_decode_f32_noalloc": (C.c_int, [_vp, C.POINTER(Cfg), _vp, _sz, _vp, _vp, _vp, _vp]),
     "ldpc_batch_create": (C.c_int, [C.POINTER(_vp), C.POINTER(Cfg), C.c_int, C.c_int, C.POINTER(_vp)]),
     "ldpc_batch_set_offsets": (C.c_int, [_vp, C.c_int, _vp]),
@@ -151,6 +152,15 @@ def probe_fp32_peak(device: int = 0):
     f, m = C.c_double(), C.c_double()
     check(lib.ldpc_probe_fp32_peak(device, C.byref(f), C.byref(m)))
     return f.value, m.value
+
+
+def probe_op_rates(device: int = 0):
+    """[(operation, thread-level ops per clock per SM)] of the packed-lane probe."""
+    n = 17
+    v = (C.c_double * n)()
+    names = (C.c_char_p * n)()
+    check(lib.ldpc_probe_op_rates(device, v, n, names))
+    return [(names[i].decode(), v[i]) for i in range(n)]
 
 
 def _ptr(x) -> Optional[int]:
