@@ -42,6 +42,7 @@
 
 #include "codes_fixed.cuh"
 #include "tables.h"
+#include "writeout.cuh"
 
 namespace ldpc {
 
@@ -449,43 +450,25 @@ __global__ void __launch_bounds__(MAXT, MINB) oms_f16_kernel(const __grid_consta
                 continue;
             }
             __half* pk = reinterpret_cast<__half*>(Ps + gg * stride) + hsel;
-            // hard decisions of the data columns, 32 per ballot
+            // hard decisions of the data columns, 32 per ballot; error counts
             const uint32_t* ref = job.ref_bits ? job.ref_bits + (cw % job.ref_period) * tb.hard_words : nullptr;
-            uint32_t mine = 0, refw = 0, errw = 0;
-            unsigned errslots = 0;
-            for (int w0 = 0; w0 < tb.hard_words; w0 += 32) {
-                if (ref && w0 + lane < tb.hard_words) refw = ref[w0 + lane];
-                const int wn = min(32, tb.hard_words - w0);
-                for (int w = 0; w < wn; ++w) {
-                    const int i = (w0 + w) * 32 + lane;
-                    const bool b = (i < tb.kbits) && __hlt(pk[2 * i], __float2half(0.0f));
-                    const uint32_t word = __ballot_sync(0xffffffffu, b);
-                    if (lane == w) mine = word;
-                    if (ref) {
-                        const uint32_t rw = __shfl_sync(0xffffffffu, refw, w);
-                        const bool e = (i < tb.kbits) && (b != (bool)((rw >> lane) & 1u));
-                        if (e) errslots |= 1u << ((i % z) % job.num_par);
-                        errw += __popc(__ballot_sync(0xffffffffu, e));
-                    }
-                }
-                if (job.hard_out && lane < wn) job.hard_out[cw * tb.hard_words + w0 + lane] = mine;
-            }
+            unsigned errw, errslots;
+            warp_hard_decisions([&](int i) { return __hlt(pk[2 * i], __float2half(0.0f)); }, tb.kbits, tb.hard_words, z,
+                                job.num_par, job.hard_out ? job.hard_out + cw * tb.hard_words : nullptr, ref, lane, errw,
+                                errslots);
             if (job.post_out) {
                 int8_t* dst = job.post_out + cw * (long long)n;
                 for (int i = lane; i < n; i += 32) dst[i] = (int8_t)__half2int_rn(pk[2 * i]);
             }
             if (lane == 0 && job.iters_out) job.iters_out[cw] = (uint8_t)it;
-            if (job.counters) {
-                const unsigned slots = __reduce_or_sync(0xffffffffu, errslots);
-                if (lane == 0) {
-                    int bk = (int)(cw / job.bucket_size);
-                    bk = bk < job.n_buckets ? bk : job.n_buckets - 1;
-                    atomicAdd(&s_cnt[bk][0], 1ull);
-                    atomicAdd(&s_cnt[bk][1], (unsigned long long)it);
-                    if (errw) {
-                        atomicAdd(&s_cnt[bk][2], (unsigned long long)errw);
-                        atomicAdd(&s_cnt[bk][3], (unsigned long long)__popc(slots));
-                    }
+            if (job.counters && lane == 0) {
+                int bk = (int)(cw / job.bucket_size);
+                bk = bk < job.n_buckets ? bk : job.n_buckets - 1;
+                atomicAdd(&s_cnt[bk][0], 1ull);
+                atomicAdd(&s_cnt[bk][1], (unsigned long long)it);
+                if (errw) {
+                    atomicAdd(&s_cnt[bk][2], (unsigned long long)errw);
+                    atomicAdd(&s_cnt[bk][3], (unsigned long long)__popc(errslots));
                 }
             }
             __syncwarp();

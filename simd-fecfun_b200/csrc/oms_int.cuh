@@ -217,41 +217,22 @@ __global__ void __launch_bounds__(512) oms_int_kernel(const __grid_constant__ Sp
             }
             const int32_t* pk = Ps + k * stride;
             const uint32_t* ref = job.ref_bits ? job.ref_bits + (cw % job.ref_period) * tb.hard_words : nullptr;
-            uint32_t mine = 0, refw = 0, errw = 0;
-            unsigned errslots = 0;
-            for (int w0 = 0; w0 < tb.hard_words; w0 += 32) {
-                if (ref && w0 + lane < tb.hard_words) refw = ref[w0 + lane];
-                const int wn = min(32, tb.hard_words - w0);
-                for (int w = 0; w < wn; ++w) {
-                    const int i = (w0 + w) * 32 + lane;
-                    const bool b = (i < tb.kbits) && (pk[i] < 0);
-                    const uint32_t word = __ballot_sync(0xffffffffu, b);
-                    if (lane == w) mine = word;
-                    if (ref) {
-                        const uint32_t rw = __shfl_sync(0xffffffffu, refw, w);
-                        const bool er = (i < tb.kbits) && (b != (bool)((rw >> lane) & 1u));
-                        if (er) errslots |= 1u << ((i % z) % job.num_par);
-                        errw += __popc(__ballot_sync(0xffffffffu, er));
-                    }
-                }
-                if (job.hard_out && lane < wn) job.hard_out[cw * tb.hard_words + w0 + lane] = mine;
-            }
+            unsigned errw, errslots;
+            warp_hard_decisions([&](int i) { return pk[i] < 0; }, tb.kbits, tb.hard_words, z, job.num_par,
+                                job.hard_out ? job.hard_out + cw * tb.hard_words : nullptr, ref, lane, errw, errslots);
             if (job.post_out) {
                 TL* dst = reinterpret_cast<TL*>(job.post_out) + cw * (long long)n;
                 for (int i = lane; i < n; i += 32) dst[i] = (TL)pk[i];
             }
             if (lane == 0 && job.iters_out) job.iters_out[cw] = (uint8_t)it;
-            if (job.counters) {
-                const unsigned slots = __reduce_or_sync(0xffffffffu, errslots);
-                if (lane == 0) {
-                    int bk = (int)(cw / job.bucket_size);
-                    bk = bk < job.n_buckets ? bk : job.n_buckets - 1;
-                    atomicAdd(&s_cnt[bk][0], 1ull);
-                    atomicAdd(&s_cnt[bk][1], (unsigned long long)it);
-                    if (errw) {
-                        atomicAdd(&s_cnt[bk][2], (unsigned long long)errw);
-                        atomicAdd(&s_cnt[bk][3], (unsigned long long)__popc(slots));
-                    }
+            if (job.counters && lane == 0) {
+                int bk = (int)(cw / job.bucket_size);
+                bk = bk < job.n_buckets ? bk : job.n_buckets - 1;
+                atomicAdd(&s_cnt[bk][0], 1ull);
+                atomicAdd(&s_cnt[bk][1], (unsigned long long)it);
+                if (errw) {
+                    atomicAdd(&s_cnt[bk][2], (unsigned long long)errw);
+                    atomicAdd(&s_cnt[bk][3], (unsigned long long)__popc(errslots));
                 }
             }
             __syncwarp();

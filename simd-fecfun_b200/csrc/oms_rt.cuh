@@ -177,7 +177,11 @@ __device__ __forceinline__ void rt_slots_coop(const RtCode& C, const RtJob& job,
                 uint32_t e = word ^ ref[i0 >> 5];
                 if (i0 + 32 > C.kbits) e &= (1u << (C.kbits - i0)) - 1u;
                 errw += __popc(e);
-                if ((e >> lane) & 1u) errslots |= 1u << ((i % z) % C.num_par);
+                if (C.num_par == 1) {
+                    if (e) errslots = 1u;
+                } else if ((e >> lane) & 1u) {
+                    errslots |= 1u << ((i % z) % C.num_par);
+                }
             }
         }
         if (ref && job.counters) {
@@ -389,41 +393,23 @@ __global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtL
                 }
                 __half* pk = reinterpret_cast<__half*>(Ps + gg * stride) + hsel;
                 const uint32_t* ref = job.ref_bits ? job.ref_bits + (cw % job.ref_period) * C.hard_words : nullptr;
-                uint32_t mine = 0, refw = 0, errw = 0;
-                unsigned errslots = 0;
-                for (int w0 = 0; w0 < C.hard_words; w0 += 32) {
-                    if (ref && w0 + lane < C.hard_words) refw = ref[w0 + lane];
-                    const int wn = min(32, C.hard_words - w0);
-                    for (int w = 0; w < wn; ++w) {
-                        const int i = (w0 + w) * 32 + lane;
-                        const bool b = (i < C.kbits) && __hlt(pk[2 * i], __float2half(0.0f));
-                        const uint32_t word = __ballot_sync(0xffffffffu, b);
-                        if (lane == w) mine = word;
-                        if (ref) {
-                            const uint32_t rw = __shfl_sync(0xffffffffu, refw, w);
-                            const bool e = (i < C.kbits) && (b != (bool)((rw >> lane) & 1u));
-                            if (e) errslots |= 1u << ((i % z) % C.num_par);
-                            errw += __popc(__ballot_sync(0xffffffffu, e));
-                        }
-                    }
-                    if (job.hard_out && lane < wn) job.hard_out[cw * C.hard_words + w0 + lane] = mine;
-                }
+                unsigned errw, errslots;
+                warp_hard_decisions([&](int i) { return __hlt(pk[2 * i], __float2half(0.0f)); }, C.kbits, C.hard_words, z,
+                                    C.num_par, job.hard_out ? job.hard_out + cw * C.hard_words : nullptr, ref, lane, errw,
+                                    errslots);
                 if (job.post_out) {
                     int8_t* dst = job.post_out + cw * (long long)n;
                     for (int i = lane; i < n; i += 32) dst[i] = (int8_t)__half2int_rn(pk[2 * i]);
                 }
                 if (lane == 0 && job.iters_out) job.iters_out[cw] = (uint8_t)it;
-                if (job.counters) {
-                    const unsigned slots = __reduce_or_sync(0xffffffffu, errslots);
-                    if (lane == 0) {
-                        int bk = (int)(cw / job.bucket_size);
-                        bk = bk < job.n_buckets ? bk : job.n_buckets - 1;
-                        atomicAdd(&s_cnt[bk][0], 1ull);
-                        atomicAdd(&s_cnt[bk][1], (unsigned long long)it);
-                        if (errw) {
-                            atomicAdd(&s_cnt[bk][2], (unsigned long long)errw);
-                            atomicAdd(&s_cnt[bk][3], (unsigned long long)__popc(slots));
-                        }
+                if (job.counters && lane == 0) {
+                    int bk = (int)(cw / job.bucket_size);
+                    bk = bk < job.n_buckets ? bk : job.n_buckets - 1;
+                    atomicAdd(&s_cnt[bk][0], 1ull);
+                    atomicAdd(&s_cnt[bk][1], (unsigned long long)it);
+                    if (errw) {
+                        atomicAdd(&s_cnt[bk][2], (unsigned long long)errw);
+                        atomicAdd(&s_cnt[bk][3], (unsigned long long)__popc(errslots));
                     }
                 }
                 __syncwarp();

@@ -72,7 +72,12 @@ __device__ __forceinline__ uint32_t op_apply(int op, uint32_t a, uint32_t b) {
         case 10: asm("fma.rn.f16x2 %0, %1, %2, %1;" : "=r"(d) : "r"(a), "r"(b)); break;
         case 11: asm("min.xorsign.abs.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); break;
         case 12: asm("set.eq.u32.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b)); d ^= a; break;
-        case 13: d = __float_as_uint(fminf(__uint_as_float(a), __uint_as_float(b))); break;
+        case 13: {
+            float f;
+            asm volatile("min.f32 %0, %1, %2;" : "=f"(f) : "f"(__uint_as_float(a)), "f"(__uint_as_float(b)));
+            d = __float_as_uint(f);
+            break;
+        }
         case 14: d = __float_as_uint(__fadd_rn(__uint_as_float(a), __uint_as_float(b))); break;
         case 15: d = __byte_perm(a, b, 0x5410); break;
         default: asm("lop3.b32 %0, %1, %2, %1, 0x96;" : "=r"(d) : "r"(a), "r"(b)); break;
