@@ -453,7 +453,7 @@ __global__ void __launch_bounds__(MAXT, MINB) oms_f16_kernel(const __grid_consta
             // hard decisions of the data columns, 32 per ballot; error counts
             const uint32_t* ref = job.ref_bits ? job.ref_bits + (cw % job.ref_period) * tb.hard_words : nullptr;
             unsigned errw, errslots;
-            warp_hard_decisions([&](int i) { return __hlt(pk[2 * i], __float2half(0.0f)); }, tb.kbits, tb.hard_words, z,
+            warp_hard_decisions<false>([&](int i) { return __hlt(pk[2 * i], __float2half(0.0f)); }, tb.kbits, tb.hard_words, z,
                                 job.num_par, job.hard_out ? job.hard_out + cw * tb.hard_words : nullptr, ref, lane, errw,
                                 errslots);
             if (job.post_out) {

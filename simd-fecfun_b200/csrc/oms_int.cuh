@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(512) oms_int_kernel(const __grid_constant__ Sp
             const int32_t* pk = Ps + k * stride;
             const uint32_t* ref = job.ref_bits ? job.ref_bits + (cw % job.ref_period) * tb.hard_words : nullptr;
             unsigned errw, errslots;
-            warp_hard_decisions([&](int i) { return pk[i] < 0; }, tb.kbits, tb.hard_words, z, job.num_par,
+            warp_hard_decisions<true>([&](int i) { return pk[i] < 0; }, tb.kbits, tb.hard_words, z, job.num_par,
                                 job.hard_out ? job.hard_out + cw * tb.hard_words : nullptr, ref, lane, errw, errslots);
             if (job.post_out) {
                 TL* dst = reinterpret_cast<TL*>(job.post_out) + cw * (long long)n;

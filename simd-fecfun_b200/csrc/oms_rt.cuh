@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtL
                 __half* pk = reinterpret_cast<__half*>(Ps + gg * stride) + hsel;
                 const uint32_t* ref = job.ref_bits ? job.ref_bits + (cw % job.ref_period) * C.hard_words : nullptr;
                 unsigned errw, errslots;
-                warp_hard_decisions([&](int i) { return __hlt(pk[2 * i], __float2half(0.0f)); }, C.kbits, C.hard_words, z,
+                warp_hard_decisions<false>([&](int i) { return __hlt(pk[2 * i], __float2half(0.0f)); }, C.kbits, C.hard_words, z,
                                     C.num_par, job.hard_out ? job.hard_out + cw * C.hard_words : nullptr, ref, lane, errw,
                                     errslots);
                 if (job.post_out) {

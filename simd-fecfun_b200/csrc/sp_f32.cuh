@@ -215,7 +215,7 @@ __device__ __forceinline__ void sp_decode_range(const SpTables& tb, const SpJobT
             const T* pk = Ps + k * stride;
             const uint32_t* ref = job.ref_bits ? job.ref_bits + (cw % job.ref_period) * tb.hard_words : nullptr;
             unsigned errw, errslots;
-            warp_hard_decisions([&](int i) { return pk[i] < T(0); }, tb.kbits, tb.hard_words, z, job.num_par,
+            warp_hard_decisions<true>([&](int i) { return pk[i] < T(0); }, tb.kbits, tb.hard_words, z, job.num_par,
                                 job.hard_out ? job.hard_out + cw * tb.hard_words : nullptr, ref, lane, errw, errslots);
             if (job.post_out) {
                 T* dst = job.post_out + cw * (long long)n;

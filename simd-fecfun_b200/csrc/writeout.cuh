@@ -19,14 +19,31 @@ namespace ldpc {
 // hard_dst: the codeword's hard-decision words, or null; ref: its sent data
 // words, or null (no counting).  Returns (in every lane) the bit errors in
 // errw and the set of failing sub-codeword slots in errslots.
-template <class NegF>
+// PRELOAD: load the sent words of the first two rounds before the ballots
+// (their latency then overlaps the ballots).  Measured: +3.8 % for the float
+// decoder on 802.16e Z=96 (36 words, one codeword per CTA), -0.6 % for the
+// int8 decoder on 802.11ad (11 words), which loads each round's words after
+// its ballots.
+template <bool PRELOAD, class NegF>
 __device__ __forceinline__ void warp_hard_decisions(NegF neg, int kbits, int hard_words, int z, int num_par,
                                                     uint32_t* hard_dst, const uint32_t* ref, int lane,
                                                     unsigned& errw, unsigned& errslots) {
     errw = 0;
     errslots = 0;
+    uint32_t sent_next = 0, sent_after = 0;
+    if (PRELOAD) {
+        sent_next = (ref && lane < hard_words) ? ref[lane] : 0u;
+        sent_after = (ref && 32 + lane < hard_words) ? ref[32 + lane] : 0u;
+    }
     for (int w0 = 0; w0 < hard_words; w0 += 32) {
         const int wn = min(32, hard_words - w0);
+        const bool own = lane < wn;
+        uint32_t sent = 0;
+        if (PRELOAD) {
+            sent = sent_next;
+            sent_next = sent_after;
+            sent_after = (ref && w0 + 64 + lane < hard_words) ? ref[w0 + 64 + lane] : 0u;
+        }
         uint32_t mine = 0;
 #pragma unroll 4
         for (int w = 0; w < wn; ++w) {
@@ -34,11 +51,11 @@ __device__ __forceinline__ void warp_hard_decisions(NegF neg, int kbits, int har
             const uint32_t word = __ballot_sync(0xffffffffu, (i < kbits) && neg(i));
             if (lane == w) mine = word;
         }
-        const bool own = lane < wn;
         if (hard_dst && own) hard_dst[w0 + lane] = mine;
         if (ref) {
+            if (!PRELOAD) sent = own ? ref[w0 + lane] : 0u;
             const int lo = (w0 + lane) * 32;
-            uint32_t e = own ? (mine ^ ref[w0 + lane]) : 0u;
+            uint32_t e = own ? (mine ^ sent) : 0u;
             if (own && lo + 32 > kbits) e &= (1u << (kbits - lo)) - 1u;
             errw += __reduce_add_sync(0xffffffffu, __popc(e));
             unsigned slots = 0;
