@@ -347,7 +347,10 @@ __global__ void __launch_bounds__(MAXT, MINB) oms_f16_kernel(const __grid_consta
     extern __shared__ uint32_t Ps[];
     __shared__ long long s_cur[32];      // codeword decoded by slot (-1 = none)
     __shared__ long long s_next[32];     // codeword prefetched for the slot (-1 = none)
-    __shared__ int s_it[32];
+    // iterations done by slot k (-1 = empty), one copy per iteration parity:
+    // the slot phase of parity p reads s_it[p] and writes s_it[p ^ 1], so
+    // every warp sees the same slot states while others update them
+    __shared__ int s_it[2][32];
     // per iteration parity p: failing-check bits and R-clear masks per group, busy flag
     __shared__ uint32_t s_synd[2][16];
     __shared__ uint32_t s_zero_mask[2][16];
@@ -378,7 +381,8 @@ __global__ void __launch_bounds__(MAXT, MINB) oms_f16_kernel(const __grid_consta
         const bool ok = tid < nslots;
         s_cur[tid] = ok && c0 < hi ? c0 : -1;
         s_next[tid] = ok && c1 < hi ? c1 : -1;
-        s_it[tid] = 0;
+        s_it[0][tid] = ok && c0 < hi ? 0 : -1;
+        s_it[1][tid] = -1;
         if (tid < 16) {
             s_synd[0][tid] = s_synd[1][tid] = 0;
             s_zero_mask[0][tid] = s_zero_mask[1][tid] = 0;
@@ -388,14 +392,20 @@ __global__ void __launch_bounds__(MAXT, MINB) oms_f16_kernel(const __grid_consta
     if (tid == 0) s_head = (unsigned long long)(lo + 2 * nslots);
     __syncthreads();
 
-    // initial codewords straight into the posteriors; prefetch the second round
+    // first round: through the staging buffers (16-byte copies) into the
+    // posteriors, then prefetch the second round (each warp its own slots)
+    for (int k = warp; k < nslots; k += nwarps)
+        if (s_cur[k] >= 0) prefetch_llr(stage_base + k * nstage, job.llr, s_cur[k], n, lane);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncwarp();
     for (int k = warp; k < nslots; k += nwarps) {
-        const long long cw = s_cur[k];
-        if (cw >= 0) {
+        if (s_cur[k] >= 0) {
             __half* dst = reinterpret_cast<__half*>(Ps + (k >> 1) * stride) + (k & 1);
-            const int8_t* src = job.llr + cw * (long long)n;
-            for (int i = lane; i < n; i += 32) dst[2 * i] = __int2half_rn((int)src[i]);
+            const int8_t* st = stage_base + k * nstage;
+            for (int i = lane; i < n; i += 32) dst[2 * i] = __int2half_rn((int)st[i]);
         }
+        __syncwarp();
         if (s_next[k] >= 0) prefetch_llr(stage_base + k * nstage, job.llr, s_next[k], n, lane);
     }
     cp_async_commit();
@@ -435,20 +445,31 @@ __global__ void __launch_bounds__(MAXT, MINB) oms_f16_kernel(const __grid_consta
         }
         __syncthreads();
 
-        // ====== each warp: its slots -- decide, write out, promote, claim, prefetch ======
+        // ====== slot phase: decide, write out, promote, claim, prefetch ======
         cp_async_wait_all();   // this warp's prefetches (issued an iteration ago)
         __syncwarp();
-        for (int k = warp; k < nslots; k += nwarps) {
-            const long long cw = s_cur[k];
-            if (cw < 0) continue;
-            const int gg = k >> 1, hsel = k & 1;
-            const int it = s_it[k] + 1;
-            const uint32_t bit = hsel ? 0x80000000u : 0x00008000u;
-            const bool done = !(s_synd[par][gg] & bit) || it >= job.max_iter;
-            if (!done) {
-                if (lane == 0) { s_it[k] = it; s_busy[par] = 1; }
-                continue;
+        // Lane k of every warp evaluates slot k; the finished slots are dealt
+        // out in slot order, the j-th to warp j mod nwarps, so two codewords
+        // finishing together go to different warps.
+        unsigned done_mask;
+        {
+            const int itk = lane < nslots ? s_it[par][lane] : -1;
+            const bool live = itk >= 0;
+            const uint32_t bit = (lane & 1) ? 0x80000000u : 0x00008000u;
+            const bool dn = live && (!(s_synd[par][lane >> 1] & bit) || itk + 1 >= job.max_iter);
+            done_mask = __ballot_sync(0xffffffffu, dn);
+            if (warp == 0 && lane < nslots && !dn) {
+                s_it[par ^ 1][lane] = live ? itk + 1 : -1;
+                if (live) s_busy[par] = 1;
             }
+        }
+        int j = 0;
+        for (unsigned m = done_mask; m; m &= m - 1, ++j) {
+            if (j % nwarps != warp) continue;
+            const int k = __ffs(m) - 1;
+            const long long cw = s_cur[k];
+            const int gg = k >> 1, hsel = k & 1;
+            const int it = s_it[par][k] + 1;
             __half* pk = reinterpret_cast<__half*>(Ps + gg * stride) + hsel;
             // hard decisions of the data columns, 32 per ballot; error counts
             const uint32_t* ref = job.ref_bits ? job.ref_bits + (cw % job.ref_period) * tb.hard_words : nullptr;
@@ -490,7 +511,7 @@ __global__ void __launch_bounds__(MAXT, MINB) oms_f16_kernel(const __grid_consta
             }
             if (lane == 0) {
                 s_cur[k] = nxt;
-                s_it[k] = 0;
+                s_it[par ^ 1][k] = nxt >= 0 ? 0 : -1;
                 atomicOr(&s_zero_mask[par][gg], hsel ? 0xffff0000u : 0x0000ffffu);
             }
         }

@@ -149,9 +149,11 @@ __host__ __device__ constexpr int rt_code_bytes() { return (int)((sizeof(RtCode)
 // Then, after a barrier, warp k mod nwarps does slot k's bookkeeping, claim
 // and prefetch.  Entered after a barrier that follows every thread's
 // cp.async wait; the caller commits the prefetches and ends with a barrier.
+// it_rd / it_wr: the slots' iteration counts of this iteration parity and of
+// the next (-1 = empty slot).
 __device__ __forceinline__ void rt_slots_coop(const RtCode& C, const RtJob& job, uint32_t* Ps, int8_t* stage_base, int stride,
                                            int nstage, int nslots, long long hi, int par, long long* s_cur,
-                                           long long* s_next, int* s_it, uint32_t (*s_synd)[16],
+                                           long long* s_next, const int* it_rd, int* it_wr, uint32_t (*s_synd)[16],
                                            uint32_t (*s_zero_mask)[16], int* s_busy, unsigned long long& s_head,
                                            unsigned long long (*s_cnt)[4], unsigned* s_err_bits, unsigned* s_err_slots) {
     const int tid = threadIdx.x, nthr = blockDim.x, warp = tid >> 5, lane = tid & 31, nwarps = nthr >> 5;
@@ -160,7 +162,7 @@ __device__ __forceinline__ void rt_slots_coop(const RtCode& C, const RtJob& job,
     for (int k = 0; k < nslots; ++k) {
         if (s_cur[k] < 0) continue;
         const uint32_t bit = (k & 1) ? 0x80000000u : 0x00008000u;
-        if (!(s_synd[par][k >> 1] & bit) || s_it[k] + 1 >= C.max_iter) fin |= 1u << k;
+        if (!(s_synd[par][k >> 1] & bit) || it_rd[k] + 1 >= C.max_iter) fin |= 1u << k;
     }
     for (unsigned f = fin; f; f &= f - 1) {
         const int k = __ffs(f) - 1;
@@ -200,16 +202,19 @@ __device__ __forceinline__ void rt_slots_coop(const RtCode& C, const RtJob& job,
             for (int i = tid; i < n; i += nthr) pk[2 * i] = __int2half_rn((int)st[i]);
         }
     }
-    // every thread has taken its decision from s_cur / s_it / s_synd, summed its
-    // errors and read the staging buffers before the bookkeeping changes them
+    // every thread has taken its decision from s_cur / it_rd / s_synd, summed
+    // its errors and read the staging buffers before the bookkeeping changes them
     __syncthreads();
     for (int k = warp; k < nslots; k += nwarps) {
         const long long cw = s_cur[k];
-        if (cw < 0) continue;
-        const int it = s_it[k] + 1;
+        if (cw < 0) {
+            if (lane == 0) it_wr[k] = -1;
+            continue;
+        }
+        const int it = it_rd[k] + 1;
         if (!((fin >> k) & 1u)) {
             if (lane == 0) {
-                s_it[k] = it;
+                it_wr[k] = it;
                 s_busy[par] = 1;
             }
             continue;
@@ -243,7 +248,7 @@ __device__ __forceinline__ void rt_slots_coop(const RtCode& C, const RtJob& job,
         }
         if (lane == 0) {
             s_cur[k] = nxt;
-            s_it[k] = 0;
+            it_wr[k] = nxt >= 0 ? 0 : -1;
             atomicOr(&s_zero_mask[par][k >> 1], (k & 1) ? 0xffff0000u : 0x0000ffffu);
         }
     }
@@ -254,7 +259,10 @@ __global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtL
     extern __shared__ __align__(16) unsigned char rt_smem[];
     __shared__ long long s_cur[32];
     __shared__ long long s_next[32];
-    __shared__ int s_it[32];
+    // iterations done by slot k (-1 = empty), one copy per iteration parity:
+    // the slot phase of parity p reads s_it[p] and writes s_it[p ^ 1], so
+    // every warp sees the same slot states while others update them
+    __shared__ int s_it[2][32];
     __shared__ uint32_t s_synd[2][16];
     __shared__ uint32_t s_zero_mask[2][16];
     __shared__ int s_busy[2];
@@ -325,7 +333,8 @@ __global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtL
             const bool ok = tid < nslots;
             s_cur[tid] = ok && c0 < hi ? c0 : -1;
             s_next[tid] = ok && c1 < hi ? c1 : -1;
-            s_it[tid] = 0;
+            s_it[0][tid] = ok && c0 < hi ? 0 : -1;
+            s_it[1][tid] = -1;
             s_err_bits[tid] = s_err_slots[tid] = 0;
             if (tid < 16) {
                 s_synd[0][tid] = s_synd[1][tid] = 0;
@@ -335,13 +344,20 @@ __global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtL
         }
         if (tid == 0) s_head = (unsigned long long)(lo + 2 * nslots);
         __syncthreads();
+        // first round through the staging buffers (16-byte copies), then the
+        // prefetch of the second round (each warp its own slots)
+        for (int k = warp; k < nslots; k += nwarps)
+            if (s_cur[k] >= 0) prefetch_llr(stage_base + k * nstage, job.llr, s_cur[k], n, lane);
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncwarp();
         for (int k = warp; k < nslots; k += nwarps) {
-            const long long cw = s_cur[k];
-            if (cw >= 0) {
+            if (s_cur[k] >= 0) {
                 __half* dst = reinterpret_cast<__half*>(Ps + (k >> 1) * stride) + (k & 1);
-                const int8_t* src = job.llr + cw * (long long)n;
-                for (int i = lane; i < n; i += 32) dst[2 * i] = __int2half_rn((int)src[i]);
+                const int8_t* st = stage_base + k * nstage;
+                for (int i = lane; i < n; i += 32) dst[2 * i] = __int2half_rn((int)st[i]);
             }
+            __syncwarp();
             if (s_next[k] >= 0) prefetch_llr(stage_base + k * nstage, job.llr, s_next[k], n, lane);
         }
         cp_async_commit();
@@ -350,7 +366,7 @@ __global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtL
         for (int par = 0;; par ^= 1) {
             // ---------------- one layered iteration ----------------
             // iteration index of this thread's two codewords (offset tables)
-            const int it0 = s_it[2 * g], it1 = s_it[2 * g + 1];
+            const int it0 = max(s_it[par][2 * g], 0), it1 = max(s_it[par][2 * g + 1], 0);
             for (int l = 0; l < C.L; ++l) {
                 if (active) {
                     uint32_t beta2, quirk;
@@ -373,65 +389,75 @@ __global__ void __launch_bounds__(512) oms_rt_kernel(const __grid_constant__ RtL
             if (nslots < nwarps) {
                 // ------- more warps than slots (large codes): the whole CTA writes each
                 // finished codeword out and refills its slot -------
-                rt_slots_coop(C, job, Ps, stage_base, stride, nstage, nslots, hi, par, s_cur, s_next, s_it, s_synd,
-                              s_zero_mask, s_busy, s_head, s_cnt, s_err_bits, s_err_slots);
-            } else
-            // ------- each warp: its slots -- decide, write out, promote, claim, prefetch -------
-            for (int k = warp; k < nslots; k += nwarps) {
-                const long long cw = s_cur[k];
-                if (cw < 0) continue;
-                const int gg = k >> 1, hsel = k & 1;
-                const int it = s_it[k] + 1;
-                const uint32_t bit = hsel ? 0x80000000u : 0x00008000u;
-                const bool done = !(s_synd[par][gg] & bit) || it >= C.max_iter;
-                if (!done) {
-                    if (lane == 0) {
-                        s_it[k] = it;
-                        s_busy[par] = 1;
-                    }
-                    continue;
-                }
-                __half* pk = reinterpret_cast<__half*>(Ps + gg * stride) + hsel;
-                const uint32_t* ref = job.ref_bits ? job.ref_bits + (cw % job.ref_period) * C.hard_words : nullptr;
-                unsigned errw, errslots;
-                warp_hard_decisions<false>([&](int i) { return __hlt(pk[2 * i], __float2half(0.0f)); }, C.kbits, C.hard_words, z,
-                                    C.num_par, job.hard_out ? job.hard_out + cw * C.hard_words : nullptr, ref, lane, errw,
-                                    errslots);
-                if (job.post_out) {
-                    int8_t* dst = job.post_out + cw * (long long)n;
-                    for (int i = lane; i < n; i += 32) dst[i] = (int8_t)__half2int_rn(pk[2 * i]);
-                }
-                if (lane == 0 && job.iters_out) job.iters_out[cw] = (uint8_t)it;
-                if (job.counters && lane == 0) {
-                    int bk = (int)(cw / job.bucket_size);
-                    bk = bk < job.n_buckets ? bk : job.n_buckets - 1;
-                    atomicAdd(&s_cnt[bk][0], 1ull);
-                    atomicAdd(&s_cnt[bk][1], (unsigned long long)it);
-                    if (errw) {
-                        atomicAdd(&s_cnt[bk][2], (unsigned long long)errw);
-                        atomicAdd(&s_cnt[bk][3], (unsigned long long)__popc(errslots));
+                rt_slots_coop(C, job, Ps, stage_base, stride, nstage, nslots, hi, par, s_cur, s_next, s_it[par],
+                              s_it[par ^ 1], s_synd, s_zero_mask, s_busy, s_head, s_cnt, s_err_bits, s_err_slots);
+            } else {
+                // ------- per-warp slots: lane k of every warp evaluates slot k; the
+                // finished slots are dealt out in slot order, the j-th to warp
+                // j mod nwarps (two codewords finishing together go to different
+                // warps) -------
+                unsigned done_mask;
+                {
+                    const int itk = lane < nslots ? s_it[par][lane] : -1;
+                    const bool live = itk >= 0;
+                    const uint32_t bit = (lane & 1) ? 0x80000000u : 0x00008000u;
+                    const bool dn = live && (!(s_synd[par][lane >> 1] & bit) || itk + 1 >= C.max_iter);
+                    done_mask = __ballot_sync(0xffffffffu, dn);
+                    if (warp == 0 && lane < nslots && !dn) {
+                        s_it[par ^ 1][lane] = live ? itk + 1 : -1;
+                        if (live) s_busy[par] = 1;
                     }
                 }
-                __syncwarp();
-                const long long nxt = s_next[k];
-                if (nxt >= 0) {
-                    const int8_t* st = stage_base + k * nstage;
-                    for (int i = lane; i < n; i += 32) pk[2 * i] = __int2half_rn((int)st[i]);
+                int j = 0;
+                for (unsigned m = done_mask; m; m &= m - 1, ++j) {
+                    if (j % nwarps != warp) continue;
+                    const int k = __ffs(m) - 1;
+                    const long long cw = s_cur[k];
+                    const int gg = k >> 1, hsel = k & 1;
+                    const int it = s_it[par][k] + 1;
+                    __half* pk = reinterpret_cast<__half*>(Ps + gg * stride) + hsel;
+                    const uint32_t* ref = job.ref_bits ? job.ref_bits + (cw % job.ref_period) * C.hard_words : nullptr;
+                    unsigned errw, errslots;
+                    warp_hard_decisions<false>([&](int i) { return __hlt(pk[2 * i], __float2half(0.0f)); }, C.kbits,
+                                               C.hard_words, z, C.num_par,
+                                               job.hard_out ? job.hard_out + cw * C.hard_words : nullptr, ref, lane, errw,
+                                               errslots);
+                    if (job.post_out) {
+                        int8_t* dst = job.post_out + cw * (long long)n;
+                        for (int i = lane; i < n; i += 32) dst[i] = (int8_t)__half2int_rn(pk[2 * i]);
+                    }
+                    if (lane == 0 && job.iters_out) job.iters_out[cw] = (uint8_t)it;
+                    if (job.counters && lane == 0) {
+                        int bk = (int)(cw / job.bucket_size);
+                        bk = bk < job.n_buckets ? bk : job.n_buckets - 1;
+                        atomicAdd(&s_cnt[bk][0], 1ull);
+                        atomicAdd(&s_cnt[bk][1], (unsigned long long)it);
+                        if (errw) {
+                            atomicAdd(&s_cnt[bk][2], (unsigned long long)errw);
+                            atomicAdd(&s_cnt[bk][3], (unsigned long long)__popc(errslots));
+                        }
+                    }
                     __syncwarp();
-                    unsigned long long c = 0;
-                    if (lane == 0) c = atomicAdd(&s_head, 1ull);
-                    c = __shfl_sync(0xffffffffu, c, 0);
-                    const long long fresh = (long long)c < hi ? (long long)c : -1;
-                    if (fresh >= 0) prefetch_llr(stage_base + k * nstage, job.llr, fresh, n, lane);
-                    if (lane == 0) {
-                        s_next[k] = fresh;
-                        s_busy[par] = 1;
+                    const long long nxt = s_next[k];
+                    if (nxt >= 0) {
+                        const int8_t* st = stage_base + k * nstage;
+                        for (int i = lane; i < n; i += 32) pk[2 * i] = __int2half_rn((int)st[i]);
+                        __syncwarp();
+                        unsigned long long c = 0;
+                        if (lane == 0) c = atomicAdd(&s_head, 1ull);
+                        c = __shfl_sync(0xffffffffu, c, 0);
+                        const long long fresh = (long long)c < hi ? (long long)c : -1;
+                        if (fresh >= 0) prefetch_llr(stage_base + k * nstage, job.llr, fresh, n, lane);
+                        if (lane == 0) {
+                            s_next[k] = fresh;
+                            s_busy[par] = 1;
+                        }
                     }
-                }
-                if (lane == 0) {
-                    s_cur[k] = nxt;
-                    s_it[k] = 0;
-                    atomicOr(&s_zero_mask[par][gg], hsel ? 0xffff0000u : 0x0000ffffu);
+                    if (lane == 0) {
+                        s_cur[k] = nxt;
+                        s_it[par ^ 1][k] = nxt >= 0 ? 0 : -1;
+                        atomicOr(&s_zero_mask[par][gg], hsel ? 0xffff0000u : 0x0000ffffu);
+                    }
                 }
             }
             cp_async_commit();
