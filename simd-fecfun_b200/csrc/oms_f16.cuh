@@ -462,6 +462,10 @@ __global__ void __launch_bounds__(MAXT, MINB) oms_f16_kernel(const __grid_consta
                 s_it[par ^ 1][lane] = live ? itk + 1 : -1;
                 if (live) s_busy[par] = 1;
             }
+            // no codeword finished and some slot is live: nothing below changes
+            // what the next iteration reads (its first layer barrier orders the
+            // s_it writes above), so the phase's barrier is skipped
+            if (done_mask == 0 && __any_sync(0xffffffffu, live)) continue;
         }
         int j = 0;
         for (unsigned m = done_mask; m; m &= m - 1, ++j) {
