@@ -25,6 +25,7 @@ void sigma_of(float snr, float llr_scale, float* sigma, float* sf) {
 // warp encoder, 32 codewords per tile (halved until it fits 100 KB).
 size_t gen_tile_shape(const GenTables& t, GenTile* tile) {
     const size_t nw = t.n / 32 + 3, dwp = t.kbits / 32 + 3;
+    tile->fast = tile->clamp16 = tile->qshift = 0;
     tile->thread_enc = (t.z <= 64 && !t.any_filler) ? 1 : 0;
     size_t smem = 0;
     if (tile->thread_enc) {
@@ -146,11 +147,24 @@ int launch_gen(ldpc_ctx* x, uint64_t seed, uint64_t cw_offset, const float* snr_
     job.snr_stride = (long long)n_per_snr * x->gent.n;
     // the fast path counts uncoded errors in byte counters folded once per tile:
     // at most 255 items (4-bit blocks) per thread and tile
+    // Items of 4 << qshift elements: the widest of 16, 8 and 4 that divides n and whose
+    // store (4, 8 or 16 bytes at a time) the output base alignment allows.  An item adds up to
+    // 1 << qshift to each byte counter: at most 256 - (1 << qshift) 4-bit blocks per thread and tile.
     const int nb = (x->gent.n + 3) / 4;
+    tile.qshift = 0;
     if (tile.fast) {
-        if (nb > 255 * GEN_THREADS) tile.fast = 0;
+        const uintptr_t al = (uintptr_t)job.llr_i8;
+        for (int q = GEN_MAX_QSHIFT; q > 0; --q) {
+            const int w = 4 << q;
+            if (x->gent.n % w == 0 && (al % (uintptr_t)std::min(w, 16)) == 0) {
+                tile.qshift = q;
+                break;
+            }
+        }
+        const long long cap = (256LL - (1LL << tile.qshift)) * GEN_THREADS;
+        if (nb > cap) tile.fast = tile.qshift = 0;
         else
-            while (tile.T > 1 && (long long)tile.T * nb > 255LL * GEN_THREADS) tile.T /= 2;
+            while (tile.T > 1 && (long long)tile.T * nb > cap) tile.T /= 2;
     }
     const bool pf = x->gent.any_punct || x->gent.any_filler;
     const void* kfn = pf ? (const void*)gen_kernel<true> : (const void*)gen_kernel<false>;
