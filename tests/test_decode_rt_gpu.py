@@ -68,16 +68,18 @@ def test_forced_runtime_kernel(capi, oracle, env, name, snr):
     _check(capi, oracle, code, llr, env=env)
 
 
+@pytest.mark.parametrize("env", [None, {"LDPC_OMS_RT": "1", "LDPC_OMS_RT_GLOBAL": "1"}], ids=["default", "rt_global"])
 @pytest.mark.parametrize("beta,mrm,max_iter", [(0.0, 31.0, 10), (2.0, 20.0, 7), (1.0, 127.0, 1), (0.0, 5e-8, 10)])
-def test_runtime_parameters_and_saturation(capi, oracle, beta, mrm, max_iter):
-    """beta = 0 (the abs8(-128) quirk), clamps, max_iter = 1, full-range LLRs."""
+def test_runtime_parameters_and_saturation(capi, oracle, beta, mrm, max_iter, env):
+    """beta = 0 (the abs8(-128) quirk), clamps, max_iter = 1, full-range LLRs;
+    the default kernel and the run-time-table kernel with global messages."""
     from ldpc_b200 import codes
     code = codes.code_by_name("5GNR_n1000_k500")
     llr, _, _ = make_llr_int8(code, 300, -1.0, seed=21, max_abs=100.0, scale=8.0, oracle=oracle)
-    _check(capi, oracle, code, llr, max_iter=max_iter, mrm=mrm, beta=beta)
+    _check(capi, oracle, code, llr, max_iter=max_iter, mrm=mrm, beta=beta, env=env)
     rng = np.random.default_rng(4)
     big = np.where(rng.random((200, code.n)) < 0.5, -128, 127).astype(np.int8)
-    _check(capi, oracle, code, big, max_iter=max_iter, mrm=mrm, beta=beta)
+    _check(capi, oracle, code, big, max_iter=max_iter, mrm=mrm, beta=beta, env=env)
 
 
 @pytest.mark.parametrize("n", [1, 5, 33, 1001])
