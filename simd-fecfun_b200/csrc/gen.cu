@@ -57,7 +57,8 @@ int setup_gen(ldpc_ctx* x) {
     const ldpc_code& c = x->code;
     GenTables& t = x->gent;
     memset(&t, 0, sizeof(t));
-    if (c.mrow > GEN_MAX_PAR || (int)c.term_col.size() > GEN_MAX_TERMS || c.mcol > GEN_MAX_COLS)
+    // terms beyond the parameter block go to device memory; par_first is 16 bits
+    if (c.mrow > GEN_MAX_PAR || (int)c.term_col.size() > 32767 || c.mcol > GEN_MAX_COLS)
         return fail(LDPC_ERR_UNSUPPORTED, "encoder schedule too large (%d parity columns, %zu terms)", c.mrow,
                     c.term_col.size());
     t.z = c.z;
@@ -73,9 +74,21 @@ int setup_gen(ldpc_ctx* x) {
         t.par_first[i] = (int16_t)c.sched_first[i];
         t.par_cnt[i] = (int16_t)c.sched_cnt[i];
     }
-    for (size_t k = 0; k < c.term_col.size(); ++k) {
-        t.term_col[k] = (int16_t)c.term_col[k];
-        t.term_shift[k] = (int16_t)c.term_shift[k];
+    t.n_terms = (int)c.term_col.size();
+    if (t.n_terms <= GEN_MAX_TERMS) {
+        for (size_t k = 0; k < c.term_col.size(); ++k) {
+            t.term_col[k] = (int16_t)c.term_col[k];
+            t.term_shift[k] = (int16_t)c.term_shift[k];
+        }
+    } else {
+        std::vector<int16_t> h(2 * (size_t)t.n_terms);
+        for (int k = 0; k < t.n_terms; ++k) {
+            h[k] = (int16_t)c.term_col[k];
+            h[t.n_terms + k] = (int16_t)c.term_shift[k];
+        }
+        CUDA_TRY(cudaMalloc(&x->d_gen_terms, h.size() * sizeof(int16_t)));
+        CUDA_TRY(cudaMemcpy(x->d_gen_terms, h.data(), h.size() * sizeof(int16_t), cudaMemcpyHostToDevice));
+        t.term_dev = x->d_gen_terms;
     }
     t.any_punct = std::any_of(c.punct.begin(), c.punct.end(), [](uint8_t v) { return v != 0; });
     t.any_filler = std::any_of(c.filler.begin(), c.filler.end(), [](uint8_t v) { return v != 0; });
@@ -99,6 +112,8 @@ int setup_gen(ldpc_ctx* x) {
 void release_gen(ldpc_ctx* x) {
     cudaFree(x->d_masks);
     x->d_masks = nullptr;
+    cudaFree(x->d_gen_terms);
+    x->d_gen_terms = nullptr;
     cudaFree(x->d_sim_llr);
     cudaFree(x->d_sim_data);
     cudaFree(x->d_sim_hard);

@@ -26,6 +26,15 @@
 
 namespace ldpc {
 
+// Term i of the encoder schedule (parameter block, or device memory for
+// schedules longer than GEN_MAX_TERMS).
+__device__ __forceinline__ int gen_term_col(const GenTables& tb, int i) {
+    return tb.term_dev ? tb.term_dev[i] : tb.term_col[i];
+}
+__device__ __forceinline__ int gen_term_shift(const GenTables& tb, int i) {
+    return tb.term_dev ? tb.term_dev[tb.n_terms + i] : tb.term_shift[i];
+}
+
 __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
@@ -119,8 +128,8 @@ __device__ void encode_warp(const GenTables& tb, uint32_t* data, uint32_t* cols,
         for (int k = lane; k < zw; k += 32) {
             uint32_t acc = 0;
             for (int q = 0; q < cnt; ++q) {
-                const int col = tb.term_col[first + q];
-                int p = 32 * k + tb.term_shift[first + q];
+                const int col = gen_term_col(tb, first + q);
+                int p = 32 * k + gen_term_shift(tb, first + q);
                 p = p % z;
                 acc ^= col_bits32(cols + col * (zw + 1), z, p);
             }
@@ -204,7 +213,8 @@ __device__ void gen_encode_thread(const GenTables& tb, const uint32_t* dat, uint
     for (int r = 0; r < tb.n_par; ++r) {
         const int first = tb.par_first[r], cnt = tb.par_cnt[r];
         uint64_t acc = 0;
-        for (int q = 0; q < cnt; ++q) acc ^= rotr_z(cols[tb.term_col[first + q] * T + t], tb.term_shift[first + q] % z, z, mask);
+        for (int q = 0; q < cnt; ++q)
+            acc ^= rotr_z(cols[gen_term_col(tb, first + q) * T + t], gen_term_shift(tb, first + q) % z, z, mask);
         cols[tb.par_col[r] * T + t] = acc;
     }
     for (int w = 0; w < nw; ++w) bits[w * T + t] = 0u;

@@ -126,6 +126,7 @@ struct ldpc_ctx {
     bool gen_ok = false;                        // generator/encoder usable for this code
     std::string gen_err;
     uint8_t* d_masks = nullptr;                 // punct[n] then filler[n]
+    int16_t* d_gen_terms = nullptr;             // encoder schedule terms beyond the parameter block's capacity
     void* d_sim_llr = nullptr;                  // ldpc_simulate scratch: LLRs of one chunk, all SNR points
     void* d_sim_data = nullptr;                 //   sent data bits of the chunk
     void* d_sim_hard = nullptr;

@@ -144,6 +144,10 @@ struct GenTables {
     int16_t par_cnt[GEN_MAX_PAR];
     int16_t term_col[GEN_MAX_TERMS];
     int16_t term_shift[GEN_MAX_TERMS];
+    // schedules of more than GEN_MAX_TERMS terms (802.3ca's dense inverse):
+    // the terms in device memory, [n_terms] columns then [n_terms] shifts
+    const int16_t* term_dev;
+    int n_terms;
     const uint8_t* punct;            // [n] 0/1, device
     const uint8_t* filler;           // [n] 0/1, device
     int any_punct, any_filler;

@@ -68,6 +68,18 @@ def test_forced_runtime_kernel(capi, oracle, env, name, snr):
     _check(capi, oracle, code, llr, env=env)
 
 
+@pytest.mark.parametrize("name,snr", [("16e 1/2", 1.0), ("11n 5/6 z81", 4.5), ("ITU G.hn 1/2 z14", 1.0),
+                                      ("11ad 13/16", 3.4)])
+def test_padded_register_shapes(capi, oracle, name, snr):
+    """The padded register shapes (PaddedShape<L, D>), which run only when
+    LDPC_OMS_PADDED asks for them (the run-time-table kernel is the faster
+    default for these codes)."""
+    from ldpc_b200 import codes
+    code = codes.make_code(name)
+    llr, _, _ = make_llr_int8(code, 500, snr, seed=9, oracle=oracle)
+    _check(capi, oracle, code, llr, env={"LDPC_OMS_PADDED": "1"})
+
+
 @pytest.mark.parametrize("env", [None, {"LDPC_OMS_RT": "1", "LDPC_OMS_RT_GLOBAL": "1"}], ids=["default", "rt_global"])
 @pytest.mark.parametrize("beta,mrm,max_iter", [(0.0, 31.0, 10), (2.0, 20.0, 7), (1.0, 127.0, 1), (0.0, 5e-8, 10)])
 def test_runtime_parameters_and_saturation(capi, oracle, beta, mrm, max_iter, env):

@@ -8,8 +8,9 @@ from conftest import pack_bits
 
 pytestmark = pytest.mark.gpu
 
+# 802.3ca: 22355 schedule terms (its dense inverse), read from device memory
 CODES = ["11ad 1/2", "11ad 13/16", "11ay 13/16", "16e 1/2", "16e 5/6", "11n 1/2 z27", "11n 3/4 z81",
-         "ITU G.hn 1/2 z14"]
+         "ITU G.hn 1/2 z14", "802.3ca"]
 
 
 def _ctx(capi, code, **kw):
@@ -175,14 +176,14 @@ def test_integer_llrs_match_reference_gen_metrics(capi, variant, bits, scale, ma
 
 @pytest.mark.parametrize("name,n", [("11ad 1/2", 3000), ("16e 1/2", 2000), ("11n 5/6 z81", 1500),
                                     ("5GNR_n3136_k576", 1000), ("5GNR_n1000_k500", 1000), ("5GNR_n25344_k8448", 120),
-                                    ("5GNR_n2048_k704 bg1 z32", 1000)])
+                                    ("5GNR_n2048_k704 bg1 z32", 1000), ("802.3ca", 64)])
 def test_generate_int8_path_matches_float_path(capi, name, n):
     """The generator's int8-only path (four LLRs rounded and packed per word,
     uncoded errors from sign masks) against its general path on the same
     seed: identical data bits and uncoded counts, and int8 LLRs equal to the
     float LLRs rounded half-even.  Covers the per-thread encoder (Z <= 64, no
-    filler bits), the warp encoder (larger Z or filler bits), puncturing and
-    filler LLRs."""
+    filler bits), the warp encoder (larger Z or filler bits, and 802.3ca's
+    schedule in device memory), puncturing and filler LLRs."""
     import torch
     from ldpc_b200 import codes
     if name.endswith("bg1 z32"):   # Z = 32 without filler bits: the per-thread encoder with puncturing
