@@ -400,6 +400,8 @@ def run_workload(args):
                "rates": {k: round(v, 2) for k, v in rates},
                "int32_ops_per_s": capi.probe_int32_peak(local), "fp32_fma_per_s": fma, "mufu_per_s": mufu,
                "gpu_launches": None}
+    elif args.workload == "kernel-choice":
+        out = workloads.kernel_choice()
     elif args.workload == "offset-search":
         out = workloads.offset_search(n_search=args.search_n, n_valid=args.search_valid_n)
     else:
@@ -430,7 +432,7 @@ def main():
                     help="int8 codewords per host thread for the reference builds (--workload variants)")
     ap.add_argument("--workload", default="11ad",
                     choices=["11ad", "nr-mix", "hetero-mix", "learned", "sp-sweep", "variants", "sim", "offset-search",
-                             "op-rates"],
+                             "op-rates", "kernel-choice"],
                     help="11ad: the headline run; others: the batched 5G NR mix, the 18-code 802.11 mix "
                          "(plain vs learned offsets), learned-offset training, the float sum-product Z sweep, "
                          "every decoder variant on the headline point, the process-level drop-in against the "

@@ -651,3 +651,61 @@ def offset_search(snr_db=(0.0, -0.5), n_search: int = 4_000_000, n_valid: int = 
         "points": points,
         "gpu_launches": n_evals,
     }
+
+
+def kernel_choice(max_n: int = 1_000_000, llr_bytes: float = 4e8, seed: int = 5, reps: int = 3) -> Dict:
+    """int8 decode rate of every named code (802.3ca aside: one decode of it
+    outlasts the rest) with the library's kernel choice and with the padded
+    register shapes (``LDPC_OMS_PADDED``, the choice for codes without a
+    compiled shape before the run-time-table kernel replaced them), at Es/N0
+    calibrated to CWER ~1e-3; ldpc_decode_count, best of ``reps`` launches."""
+    import os
+    s = torch.cuda.current_stream()
+    per_code = {}
+    for name in [k for k in codes.ENCODE_METHOD if k != "802.3ca"]:
+        c = codes.make_code(name)
+        h = capi.Code.from_tables(c)
+        snr = _calibrate(h, c, n=20_000)
+        n = max(20_000, min(max_n, int(llr_bytes // c.n)))
+        specs, _ = _build_jobs([h], [c], [n], [[snr]], seed, 10)
+        sp = specs[0]
+        rates = {}
+        for tag, padded in (("default", False), ("padded", True)):
+            saved = os.environ.get("LDPC_OMS_PADDED")
+            if padded:
+                os.environ["LDPC_OMS_PADDED"] = "1"
+            else:
+                os.environ.pop("LDPC_OMS_PADDED", None)
+            try:
+                ctx = capi.Context(h, max_iter=10)
+            finally:
+                if saved is None:
+                    os.environ.pop("LDPC_OMS_PADDED", None)
+                else:
+                    os.environ["LDPC_OMS_PADDED"] = saved
+            best = float("inf")
+            for _ in range(reps):
+                (a, b), = _events(1)
+                a.record(s)
+                ctx.decode_count(sp["llr"], n, data_bits=sp["data_bits"], ref_period=n, bucket_size=n,
+                                 counters=sp["counters"], n_buckets=1, stream=s.cuda_stream)
+                b.record(s)
+                torch.cuda.synchronize()
+                best = min(best, a.elapsed_time(b))
+            rates[tag] = n / (best * 1e-3)
+            ctx.close()
+        per_code[name] = {"snr_db": round(snr, 3), "codewords": n, "default": rates["default"],
+                          "padded": rates["padded"], "default_over_padded": rates["default"] / rates["padded"]}
+    ratios = [v["default_over_padded"] for v in per_code.values()]
+    return {
+        "metric": "codewords/s decoded per named code, int8 offset min-sum, 10 max iterations: the library's "
+                  "kernel choice against the padded register shapes",
+        "value": None, "unit": "codewords/s", "n_gpus": 1, "higher_is_better": True, "dtype": "int8",
+        "data": "synthetic: Philox data bits, QC encoding, AWGN from the fused generator, resident in HBM",
+        "config": {"workload": "every named MatrixSet but 802.3ca; Es/N0 calibrated to CWER ~1e-3 (2e4 codewords per "
+                               "bisection point); min(%d, %.0e / N) codewords per code; best of %d launches"
+                               % (max_n, llr_bytes, reps)},
+        "default_over_padded_min_max": [min(ratios), max(ratios)],
+        "per_code": per_code,
+        "gpu_launches": None,
+    }
