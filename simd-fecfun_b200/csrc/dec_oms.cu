@@ -93,7 +93,7 @@ int setup_oms(ldpc_ctx* x) {
     // shapes without a register-resident instantiation: run-time tables.  The
     // padded shapes (PaddedShape<L, D>: 384-thread CTAs, one per SM) are slower
     // than the run-time-table kernel on every code that selects them (802.11ad
-    // 5/8 .. 13/16, 802.11ay 13/16, 802.11n, 802.16e, G.hn: 1.15-2.7x), so they
+    // 5/8 .. 13/16, 802.11ay 13/16, 802.11n, 802.16e, G.hn: 1.14-2.48x), so they
     // run only when LDPC_OMS_PADDED asks for them; the exact and compiled
     // shapes (802.11ad 1/2) stay the default.
     if (best && !best->rw && c.z <= kRtMaxThreads && !getenv("LDPC_OMS_PADDED")) return setup_oms_rt(x);
