@@ -254,11 +254,14 @@ int ldpc_batch_plan_kernels(const ldpc_batch_plan *p);
 
 /* Project autotuner: times plans over the first `sample` codewords of each
  * job (outputs not written) for every CTA width in {128..512} that fits and
- * 1, 2, 4 or 8 chunks per CTA.  It keeps the fastest setting for later plans
- * and reports it (any output pointer may be NULL).  int8 jobs of several
- * geometry classes: each class is tuned on its own jobs, and that set is
- * kept when it beats the best single shape on the whole sample; the report
- * is then the shape of the slowest class and the whole sample's time. */
+ * 1, 2, 4 or 8 chunks per CTA, and the plan that leaves every code at its
+ * own width (the single-code context's) with the default chunks per CTA.
+ * It keeps the fastest setting for later plans and reports it (any output
+ * pointer may be NULL; threads = cpc = 0 reports the codes' own widths).
+ * int8 jobs of several geometry classes: each class is tuned on its own
+ * jobs, and that set is kept when it beats the best single shape and the
+ * codes' own widths on the whole sample; the report is then the shape of
+ * the slowest class and the whole sample's time. */
 int ldpc_batch_autotune(ldpc_batch *b, const ldpc_batch_job *jobs, int n_jobs, size_t sample, int *threads,
                         int *chunks_per_cta, double *ms);
 

@@ -419,10 +419,13 @@ int int8_class(const ldpc_batch* b, int c, int threads, PlanClass* out) {
     return LDPC_OK;
 }
 
-// A code's own CTA width: int8 max(256, Z rounded to 32); float the
-// single-code context's G*Z rounded to 32, G = 128 / Z codewords per CTA.
-int default_width(const ldpc_batch* b, int z) {
-    if (b->variant == LDPC_INT8_OMS) return std::max(256, ((z + 31) / 32) * 32);
+// A code's own CTA width, the single-code context's: int8 G pairs of Z rows
+// (rt_default_G: at most 128 threads, 256 for N > 2048, fewest idle lanes),
+// float G = 128 / Z codewords per CTA; G*Z rounded to 32.
+int default_width(const ldpc_batch* b, int c) {
+    const int z = b->codes[c].z;
+    if (b->variant == LDPC_INT8_OMS)
+        return ((ldpc::rt_default_G(z, z * b->codes[c].mcol) * z + 31) / 32) * 32;
     const int G = std::max(1, std::min(32, 128 / z));
     return std::min(ldpc::kRtMaxThreads, ((G * z + 31) / 32) * 32);
 }
@@ -440,7 +443,7 @@ int plan_classes(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, bool exp
         const int c = jobs[i].code;
         if (code_cls[c] >= 0) continue;
         PlanClass k;
-        const int t = explicit_threads ? threads : default_width(b, b->codes[c].z);
+        const int t = explicit_threads ? threads : default_width(b, c);
         if (b->variant == LDPC_INT8_OMS) {
             if (int rc = int8_class(b, c, t, &k)) return rc;
         } else {
@@ -623,7 +626,7 @@ int ldpc_batch_plan_create(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs
     if (threads <= 0) threads = b->tuned_threads;
     const bool explicit_threads = threads > 0;
     if (threads <= 0) threads = std::max(256, ((maxz + 31) / 32) * 32);
-    if (cpc <= 0) cpc = b->tuned_cpc > 0 ? b->tuned_cpc : 2;
+    if (cpc <= 0) cpc = b->tuned_cpc > 0 ? b->tuned_cpc : 4;
     if (threads % 32 || threads > ldpc::kRtMaxThreads || threads < maxz)
         return fail(LDPC_ERR_UNSUPPORTED, "batch plan: %d threads per CTA (multiple of 32, >= Z=%d, <= %d)", threads, maxz,
                     ldpc::kRtMaxThreads);
@@ -823,7 +826,23 @@ int ldpc_batch_autotune(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, s
             rc = time_shape(b, sj.data(), n_jobs, 0, 0, s, e0, e1, &ms_pc);
         }
         if (rc == LDPC_OK) rc = tune_shape(b, sj.data(), n_jobs, maxz, s, e0, e1, &gt, &gc, &ms_glob);
+        // third candidate: every code at its own width with the default chunks per CTA
+        double ms_def = -1;
         if (rc == LDPC_OK) {
+            const std::vector<int> keep_t = b->code_threads, keep_c = b->code_cpc;
+            b->code_threads.clear();
+            b->code_cpc.clear();
+            rc = time_shape(b, sj.data(), n_jobs, 0, 0, s, e0, e1, &ms_def);
+            b->code_threads = keep_t;
+            b->code_cpc = keep_c;
+        }
+        if (rc == LDPC_OK && ms_def >= 0 && (ms_pc < 0 || ms_def <= ms_pc) && ms_def <= ms_glob) {
+            b->code_threads.clear();
+            b->code_cpc.clear();
+            best = ms_def;
+            best_t = 0;
+            best_c = 0;
+        } else if (rc == LDPC_OK) {
             if (ms_pc < 0 || ms_glob < ms_pc) {
                 b->tuned_threads = best_t = gt;
                 b->tuned_cpc = best_c = gc;
@@ -839,11 +858,22 @@ int ldpc_batch_autotune(ldpc_batch* b, const ldpc_batch_job* jobs, int n_jobs, s
         }
     } else if (rc == LDPC_OK) {
         rc = tune_shape(b, sj.data(), n_jobs, maxz, s, e0, e1, &best_t, &best_c, &best);
+        // against the codes' own width with the default chunks per CTA
+        double ms_def = -1;
         if (rc == LDPC_OK) {
-            b->tuned_threads = best_t;
-            b->tuned_cpc = best_c;
+            b->tuned_threads = b->tuned_cpc = 0;
             b->code_threads.clear();
             b->code_cpc.clear();
+            rc = time_shape(b, sj.data(), n_jobs, 0, 0, s, e0, e1, &ms_def);
+        }
+        if (rc == LDPC_OK) {
+            if (ms_def >= 0 && ms_def <= best) {
+                best = ms_def;
+                best_t = best_c = 0;
+            } else {
+                b->tuned_threads = best_t;
+                b->tuned_cpc = best_c;
+            }
         }
     }
     cudaEventDestroy(e0);

@@ -41,6 +41,20 @@ size_t rt_smem_bytes(int n, int G, int E, int threads, bool rsmem) {
            (rsmem ? (size_t)(E | 1) * threads * 4 : 0);   // odd per-thread stride
 }
 
+int rt_default_G(int z, int n) {
+    const int cap = n <= 2048 ? 128 : 256;
+    int G = 1;
+    double best = 0.0;
+    for (int g = 1; g <= 16 && g * z <= cap; ++g) {
+        const double eff = (double)(g * z) / (((g * z + 31) / 32) * 32);
+        if (eff >= best - 1e-9) {
+            best = eff;
+            G = g;
+        }
+    }
+    return G;
+}
+
 int rt_dmax(int d) { return d <= 8 ? 8 : d <= 12 ? 12 : d <= 16 ? 16 : d <= 24 ? 24 : d <= 32 ? 32 : 0; }
 
 int make_rt_code(const ldpc_code& c, int max_iter, uint32_t maxv2, const int* beta8, int beta8_all, int G, RtCode* out) {
@@ -97,20 +111,8 @@ int setup_oms_rt(ldpc_ctx* x) {
     // 802.16e, G.hn and 5G NR codes this is the fastest shape or within 9 %
     // of it; the former ~256-thread default for every code lost up to 35 % on
     // the short ones, a 128-thread cap up to 41 % on 5G NR base graph 2.
-    int G = 1;
-    if (const char* e = getenv("LDPC_OMS_G")) {
-        G = std::max(1, std::min(16, atoi(e)));
-    } else {
-        const int cap = n <= 2048 ? 128 : 256;
-        double best = 0.0;
-        for (int g = 1; g <= 16 && g * c.z <= cap; ++g) {
-            const double eff = (double)(g * c.z) / (((g * c.z + 31) / 32) * 32);
-            if (eff >= best - 1e-9) {
-                best = eff;
-                G = g;
-            }
-        }
-    }
+    int G = rt_default_G(c.z, n);
+    if (const char* e = getenv("LDPC_OMS_G")) G = std::max(1, std::min(16, atoi(e)));
     while (G > 1 && ((G * c.z + 31) / 32) * 32 > kRtMaxThreads) --G;
     while (G > 1 && rt_smem_bytes(n, G, E, 0, false) > (size_t)kRtMaxSmem) --G;
     const int threads = ((G * c.z + 31) / 32) * 32;

@@ -153,6 +153,9 @@ int launch_oms_rt(ldpc_ctx* x, const DecodeArgs& a, cudaStream_t s);
 int make_rt_code(const ldpc_code& c, int max_iter, uint32_t maxv2, const int* beta8, int beta8_all, int G, RtCode* out);
 // Largest row weight the run-time kernels unroll for (0: unsupported).
 int rt_dmax(int max_row_weight);
+// codeword pairs per CTA of the run-time-table kernel for a code of lift Z
+// and length N: CTAs of at most 128 threads (256 for N > 2048), fewest idle lanes
+int rt_default_G(int z, int n);
 constexpr int kRtMaxThreads = 512;          // __launch_bounds__ of oms_rt_kernel
 constexpr int kRtMaxSmem = 200 * 1024;      // dynamic shared memory the run-time kernels may use
 rt_fn rt_kernel_for(int dmax, bool quirk, bool rsmem);

@@ -223,7 +223,7 @@ def hetero_mix(steps: int = 3, warmup: int = 1, total: int = 10_000_000, seed: i
     counts = [total // len(objs) + (1 if i < total % len(objs) else 0) for i in range(len(objs))]
     specs, meta = _build_jobs(handles, objs, counts, [[s] for s in snr], seed, 10)
     batch = capi.Batch(handles, [dict(max_iter=10)] * len(objs))
-    tuned = batch.autotune(specs, sample=8192)
+    tuned = batch.autotune(specs, sample=32768)
     plan = batch.plan(specs)
     ms_plain = _time_plan(plan, specs, steps, warmup)
     q_plain = _quality(specs, meta, names, objs, steps)
