@@ -665,8 +665,7 @@ int ldpc_batch_plan_graph_launch(ldpc_batch_plan* p, void* stream) {
         for (ldpc_batch_plan* q : leaves) {
             if (!q->n_chunks) continue;
             void* arg = q->is_float ? (void*)&q->slp : (void*)&q->lp;
-            cudaKernelNodeParams kp;
-            memset(&kp, 0, sizeof(kp));
+            cudaKernelNodeParams kp{};
             kp.func = q->is_float ? q->kf : (void*)q->k;
             kp.gridDim = dim3((unsigned)q->grid);
             kp.blockDim = dim3((unsigned)q->threads);

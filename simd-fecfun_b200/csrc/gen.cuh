@@ -470,7 +470,6 @@ __global__ void __launch_bounds__(GEN_THREADS, 4) gen_kernel(const __grid_consta
             default: gen_items_fast<4, PF>(tb, job, bits, T, i0, tc, tid, tile.clamp16, unc_f);
             }
         } else {
-            const long long row_stride = tb.n;
             // (c, b) of item f advanced by GEN_THREADS items per step, without a division per item
             int c = tid / nb, b = tid - (tid / nb) * nb;
             const int step_c = GEN_THREADS / nb, step_b = GEN_THREADS - step_c * nb;
